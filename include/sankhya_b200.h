@@ -1,0 +1,183 @@
+/* Extensions of the B200 PDHG engine beyond the reference's C ABI.
+ *
+ * New symbols only; every reference signature in sankhya_cuda.h is unchanged.
+ * Settings structs carry a struct_version so later fields can be appended.
+ */
+#ifndef SANKHYA_B200_H
+#define SANKHYA_B200_H
+
+#include "sankhya_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ timing */
+
+/* Device-side timing of the most recent solve call on this thread, taken with
+   CUDA events on the engine's stream. No counterpart in the reference (its
+   benchmarks time whole calls on the host, benchmarks/bench_pdlp.cpp:131-281). */
+typedef struct SankhyaB200Timing {
+    int iterations;          /* PDHG iterations executed on the device          */
+    int checkpoints;         /* checkpoint evaluations (host-visible syncs)      */
+    int kernel_launches;     /* engine kernels launched by the call              */
+    int per_kernel_samples;  /* iterations sampled for the per-kernel averages   */
+    double loop_ms;          /* events around all iteration kernels              */
+    double checkpoint_ms;    /* events around checkpoint kernels + result copy   */
+    double dual_kernel_ms;   /* average duration of one fused A-side launch      */
+    double primal_kernel_ms; /* average duration of one fused A'-side launch     */
+    double h2d_ms;           /* input upload                                     */
+    double d2h_ms;           /* solution download                                */
+} SankhyaB200Timing;
+
+/* level 0: none; 1: loop/checkpoint/copy events; 2: also per-kernel events on
+   every iteration (adds two event records per launch). Thread-local. */
+SANKHYA_CUDA_API void sankhya_b200_set_timing(int level);
+SANKHYA_CUDA_API void sankhya_b200_last_timing(SankhyaB200Timing* out);
+
+/* --------------------------------------------------- sk_solve continuous hook */
+
+/* Layout-compatible copies of the reference's public model types
+   (c/include/sankhya.h:64-161). Skipped when that header was included first. */
+#ifndef SANKHYA_H
+typedef struct sk_csc {
+    int nrow;
+    int ncol;
+    int* p;
+    int* i;
+    double* x;
+    int nzmax;
+} sk_csc;
+
+typedef struct sk_model {
+    int nrow;
+    int ncol;
+    sk_csc A;
+    sk_csc* Q;
+    double* c;
+    double* rlow;
+    double* rupp;
+    double* clow;
+    double* cupp;
+    unsigned char* vartype;
+    double objshift;
+    double objsense;
+    char** rowname;
+    char** colname;
+    char* name;
+} sk_model;
+
+typedef struct sk_options {
+    double primal_tol;
+    double dual_tol;
+    double pivot_tol;
+    double time_limit;
+    long long iteration_limit;
+    long long node_limit;
+    int presolve;
+    int scaling;
+    int refactor_interval;
+    int verbosity;
+    int threads;
+    double mip_gap_abs;
+    double mip_gap_rel;
+    int mip_cuts;
+    int mip_heuristics;
+    int dual_simplex;
+    int lp_engine;
+    unsigned long long random_seed;
+} sk_options;
+#endif
+
+/* Output of the loop replacement below. */
+typedef struct SankhyaB200LoopResult {
+    int iterations;   /* iterations executed (the reference's performed_iterations) */
+    int converged;    /* all gates passed at a checkpoint                           */
+    int numeric_failure;
+    double dual_step; /* max |y_new - y| of the last executed iteration            */
+    double anorm;     /* sqrt(max column mass * max row mass) of A                 */
+    double seconds;
+} SankhyaB200LoopResult;
+
+/* Replaces the first-order loop of solve_continuous, c/src/sk_solve.c:849-954:
+   diagonal steps tau_j = 0.9/(1 + |A_:j|_1 + |Q_:j|_1), sigma_i = 0.9/(1 + |A_i:|_1),
+   x0 = clamp(0), y0 = 0, x_bar = 2 x_new - x, a checkpoint every 20 iterations
+   with the reference's gates (row violation <= primal_tol, max|x_bar - x| <=
+   primal_tol * max(1, |x|_inf), max|y_new - y| <= dual_tol (1 + anorm), and for
+   QP the sk_verify score <= 100 (primal_tol + 2 dual_tol)). x (ncol), y (nrow) and
+   activity (nrow) are host outputs with the reference's meaning. The time limit
+   is tested after every 20-iteration window instead of after every iteration.
+   Returns 0, SK_ERR_ARG (1) on invalid input, SK_ERR_MEMORY (2) on allocation
+   failure, SK_ERR_NUMERIC (7) on a CUDA error. */
+SANKHYA_CUDA_API int sankhya_b200_pdhg_loop(
+    const sk_model* model, const sk_options* options, double* x, double* y,
+    double* activity, SankhyaB200LoopResult* result);
+
+/* ------------------------------------------------------- restarted PDLP */
+
+enum {
+    SANKHYA_B200_SCALE_RUIZ = 1,           /* src/lp/Scaling.cpp:11-92              */
+    SANKHYA_B200_SCALE_POCK_CHAMBOLLE = 2, /* src/lp/Scaling.cpp:111-145 (alpha=1)  */
+    SANKHYA_B200_SCALE_POW2 = 4            /* c/src/sk_scale.c:20-72                */
+};
+
+enum {
+    SANKHYA_B200_FP64 = 0,       /* FP64 everywhere                                  */
+    SANKHYA_B200_FP32_REFINE = 1 /* FP32 inner iterations, FP64 refinement residuals */
+};
+
+typedef struct SankhyaB200PdlpSettings {
+    int struct_version;   /* 1 */
+    int max_iterations;   /* total PDHG iterations (accepted + rejected)          */
+    int restart_period;   /* iterations between evaluations (GpuPdlp: 64)         */
+    int power_iterations; /* power iterations for ||A||_2 (GpuPdlp: 30)           */
+    int adaptive_step;    /* 1: Applegate et al. adaptive step; 0: 0.9/||A||_2    */
+    int scaling;          /* bitmask of SANKHYA_B200_SCALE_*                      */
+    int ruiz_iterations;  /* 100                                                  */
+    int precision;        /* SANKHYA_B200_FP64 or SANKHYA_B200_FP32_REFINE        */
+    double eps_optimal;   /* relative KKT tolerance on all three measures         */
+    double time_limit;    /* seconds, <= 0 for none                               */
+    double eta_min_factor;/* 1e-6 */
+    double eta_max_factor;/* 1e4  */
+    double ruiz_tolerance;/* 1e-2 */
+} SankhyaB200PdlpSettings;
+
+SANKHYA_CUDA_API void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* settings);
+
+typedef struct SankhyaB200PdlpResult {
+    int status;            /* 0 converged, 1 iteration limit, 2 time limit, -2 numeric */
+    int iterations;
+    int restarts;
+    int rejected_steps;
+    int host_syncs;
+    int refinements;       /* outer refinement passes (FP32_REFINE)               */
+    double primal_objective;
+    double dual_objective;
+    double relative_primal_residual;
+    double relative_dual_residual;
+    double relative_gap;
+    double matrix_norm;
+    double final_step_size;
+    double primal_weight;
+    double seconds;
+} SankhyaB200PdlpResult;
+
+/* Restarted adaptive PDLP (the algorithm of the reference's GpuPdlp,
+   src/cuda/GpuPdlp.cpp:252-534) behind the C ABI: optional scaling of the
+   model, restarts at the 0.2 / 0.8 / 0.36 criteria, primal-weight smoothing,
+   relative-KKT termination. Host arrays; x0 / y0 optional warm start (NULL:
+   zeros). x_out (cols) and y_out (rows, may be NULL) are in the caller's
+   unscaled space. Bounds with magnitude >= 1e30 are absent. Returns 0, -1 on
+   invalid input or CUDA error, -2 on a non-finite iterate. */
+SANKHYA_CUDA_API int sankhya_b200_pdlp_solve(
+    const SankhyaCudaCSR* matrix, const double* c,
+    const double* row_lower, const double* row_upper,
+    const double* col_lower, const double* col_upper,
+    const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
+    double* x_out, double* y_out, SankhyaB200PdlpResult* result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

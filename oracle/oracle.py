@@ -1,0 +1,358 @@
+"""ctypes bindings for the checkers in this folder.
+
+TEST INFRASTRUCTURE ONLY. Imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py; the product never imports it.
+
+  liboracle.so                  C restatement of the reference path (pdhg_oracle.c)
+  _ref/libsankhya_ref.so        the reference's own C core (sk_solve, sk_verify, ...)
+  _ref/libsankhya_cuda_ref.so   the reference's CUDA prototype built for sm_100a
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_libs: dict[str, C.CDLL] = {}
+
+dptr = C.POINTER(C.c_double)
+iptr = C.POINTER(C.c_int)
+
+
+def _as_d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _as_i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _p(a, t=dptr):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def load(name: str) -> C.CDLL:
+    if name not in _libs:
+        path = {"oracle": os.path.join(HERE, "liboracle.so"),
+                "ref": os.path.join(HERE, "_ref", "libsankhya_ref.so"),
+                "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so")}[name]
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")
+        _libs[name] = C.CDLL(path)
+    return _libs[name]
+
+
+def available(name: str) -> bool:
+    try:
+        load(name)
+        return True
+    except (FileNotFoundError, OSError):
+        return False
+
+
+# ---------------------------------------------------------------- oracle structs
+
+class OrcCsr(C.Structure):
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("ptr", iptr), ("idx", iptr), ("val", dptr)]
+
+
+class LPSettings(C.Structure):
+    """Layout of SankhyaCudaLPSettings (and orc_settings)."""
+    _fields_ = [("max_iterations", C.c_int), ("check_every", C.c_int), ("tau", C.c_double),
+                ("sigma", C.c_double), ("theta", C.c_double), ("tolerance", C.c_double),
+                ("time_limit", C.c_double)]
+
+
+class LPResult(C.Structure):
+    """Layout of SankhyaCudaLPResult (and orc_result)."""
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("objective", C.c_double),
+                ("maximum_row_violation", C.c_double), ("maximum_step", C.c_double),
+                ("maximum_kkt_residual", C.c_double), ("maximum_dual_residual", C.c_double),
+                ("maximum_complementarity", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SkOut(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("dual_step", C.c_double),
+                ("anorm", C.c_double)]
+
+
+class Verify(C.Structure):
+    _fields_ = [("objective", C.c_double), ("primal_infeasibility", C.c_double),
+                ("dual_infeasibility", C.c_double), ("complementarity", C.c_double)]
+
+
+class PdlpParams(C.Structure):
+    _fields_ = [("eps_optimal", C.c_double), ("max_iterations", C.c_int),
+                ("restart_period", C.c_int), ("power_iterations", C.c_int),
+                ("adaptive_step", C.c_int), ("eta_min_factor", C.c_double),
+                ("eta_max_factor", C.c_double)]
+
+
+class PdlpStats(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("restarts", C.c_int),
+                ("rejected_steps", C.c_int), ("primal_objective", C.c_double),
+                ("dual_objective", C.c_double), ("relative_primal_residual", C.c_double),
+                ("relative_dual_residual", C.c_double), ("relative_gap", C.c_double),
+                ("matrix_norm", C.c_double), ("final_step_size", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class _Keep:
+    """Holds numpy buffers alive while a ctypes struct points into them."""
+
+    def __init__(self):
+        self.refs = []
+
+    def d(self, a):
+        a = _as_d(a)
+        self.refs.append(a)
+        return a
+
+    def i(self, a):
+        a = _as_i(a)
+        self.refs.append(a)
+        return a
+
+
+def _csr(keep: _Keep, rows, cols, ptr, idx, val) -> OrcCsr:
+    return OrcCsr(rows, cols, _p(keep.i(ptr), iptr), _p(keep.i(idx), iptr), _p(keep.d(val)))
+
+
+def inst_csr(keep, inst):
+    return _csr(keep, inst["m"], inst["n"], inst["ptr"], inst["idx"], inst["val"])
+
+
+def hessian_csr(keep, inst):
+    if "q_ptr" not in inst:
+        return None
+    n = inst["n"]
+    return _csr(keep, n, n, inst["q_ptr"], inst["q_idx"], inst["q_val"])
+
+
+def fixed_pdhg(inst, settings: dict, primal_steps=None, dual_steps=None, qdiag=None,
+               hessian=False, want_dual=True, **over):
+    """orc_fixed_pdhg: the cuda prototype's solve_qp restated. Returns (rc, x, y, result)."""
+    lib = load("oracle")
+    keep = _Keep()
+    a = inst_csr(keep, inst)
+    h = hessian_csr(keep, inst) if hessian else None
+    get = lambda k: keep.d(over[k]) if k in over else keep.d(inst[k])
+    x = np.zeros(inst["n"])
+    y = np.zeros(inst["m"]) if want_dual else None
+    res = LPResult()
+    s = LPSettings(**settings)
+    lib.orc_fixed_pdhg.restype = C.c_int
+    rc = lib.orc_fixed_pdhg(C.byref(a), C.byref(h) if h is not None else None,
+                            _p(keep.d(qdiag)) if qdiag is not None else None,
+                            _p(get("c")), _p(get("rl")), _p(get("ru")), _p(get("cl")), _p(get("cu")),
+                            s, _p(keep.d(primal_steps)) if primal_steps is not None else None,
+                            _p(keep.d(dual_steps)) if dual_steps is not None else None,
+                            _p(x), _p(y), C.byref(res))
+    return rc, x, y, res.as_dict()
+
+
+def sk_loop(inst, max_iterations, primal_tol=1e-7, dual_tol=1e-7, time_limit=0.0, quadratic=False):
+    lib = load("oracle")
+    keep = _Keep()
+    a = inst_csr(keep, inst)
+    q = hessian_csr(keep, inst) if quadratic else None
+    n, m = inst["n"], inst["m"]
+    x, y, act = np.zeros(n), np.zeros(m), np.zeros(m)
+    out = SkOut()
+    rc = lib.orc_sk_loop(C.byref(a), C.byref(q) if q is not None else None,
+                         _p(keep.d(inst["c"])), _p(keep.d(inst["rl"])), _p(keep.d(inst["ru"])),
+                         _p(keep.d(inst["cl"])), _p(keep.d(inst["cu"])), C.c_int(max_iterations),
+                         C.c_double(primal_tol), C.c_double(dual_tol), C.c_double(time_limit),
+                         _p(x), _p(y), _p(act), C.byref(out))
+    assert rc == 0
+    return x, y, act, {k: getattr(out, k) for k, _ in SkOut._fields_}
+
+
+def sk_verify(inst, x, y, quadratic=False, objshift=0.0):
+    lib = load("oracle")
+    keep = _Keep()
+    a = inst_csr(keep, inst)
+    q = hessian_csr(keep, inst) if quadratic else None
+    v = Verify()
+    lib.orc_sk_verify(C.byref(a), C.byref(q) if q is not None else None, _p(keep.d(inst["c"])),
+                      C.c_double(objshift), _p(keep.d(inst["rl"])), _p(keep.d(inst["ru"])),
+                      _p(keep.d(inst["cl"])), _p(keep.d(inst["cu"])), _p(keep.d(x)),
+                      _p(keep.d(y)) if y is not None else None, C.byref(v))
+    return {k: getattr(v, k) for k, _ in Verify._fields_}
+
+
+def pdlp(inst, eps=1e-8, max_iterations=100000, restart_period=64, power_iterations=30,
+         adaptive=True, eta_min_factor=1e-6, eta_max_factor=1e4):
+    lib = load("oracle")
+    keep = _Keep()
+    a = inst_csr(keep, inst)
+    p = PdlpParams(eps, max_iterations, restart_period, power_iterations, int(adaptive),
+                   eta_min_factor, eta_max_factor)
+    x, y = np.zeros(inst["n"]), np.zeros(inst["m"])
+    st = PdlpStats()
+    lib.orc_pdlp(C.byref(a), _p(keep.d(inst["c"])), _p(keep.d(inst["cl"])), _p(keep.d(inst["cu"])),
+                 _p(keep.d(inst["rl"])), _p(keep.d(inst["ru"])), C.byref(p), _p(x), _p(y),
+                 C.byref(st))
+    return x, y, st.as_dict()
+
+
+def power_norm(inst, iterations=30):
+    lib = load("oracle")
+    keep = _Keep()
+    a = inst_csr(keep, inst)
+    lib.orc_power_norm.restype = C.c_double
+    return lib.orc_power_norm(C.byref(a), C.c_int(iterations))
+
+
+def ruiz(inst, max_iters=100, tol=1e-2):
+    lib = load("oracle")
+    keep = _Keep()
+    a = inst_csr(keep, inst)
+    r, c = np.zeros(inst["m"]), np.zeros(inst["n"])
+    conv = lib.orc_ruiz(C.byref(a), C.c_int(max_iters), C.c_double(tol), _p(r), _p(c))
+    return r, c, bool(conv)
+
+
+def pock_chambolle(inst, alpha=1.0):
+    lib = load("oracle")
+    keep = _Keep()
+    a = inst_csr(keep, inst)
+    r, c = np.zeros(inst["m"]), np.zeros(inst["n"])
+    lib.orc_pock_chambolle(C.byref(a), C.c_double(alpha), _p(r), _p(c))
+    return r, c
+
+
+def pow2_scale(inst, passes=4):
+    lib = load("oracle")
+    keep = _Keep()
+    a = inst_csr(keep, inst)
+    r, c = np.zeros(inst["m"]), np.zeros(inst["n"])
+    lib.orc_pow2_scale(C.byref(a), C.c_int(passes), _p(r), _p(c))
+    return r, c
+
+
+# ------------------------------------------------------- the reference's C core
+
+class SkCsc(C.Structure):
+    _fields_ = [("nrow", C.c_int), ("ncol", C.c_int), ("p", iptr), ("i", iptr), ("x", dptr),
+                ("nzmax", C.c_int)]
+
+
+class SkModel(C.Structure):
+    _fields_ = [("nrow", C.c_int), ("ncol", C.c_int), ("A", SkCsc), ("Q", C.POINTER(SkCsc)),
+                ("c", dptr), ("rlow", dptr), ("rupp", dptr), ("clow", dptr), ("cupp", dptr),
+                ("vartype", C.POINTER(C.c_ubyte)), ("objshift", C.c_double),
+                ("objsense", C.c_double), ("rowname", C.c_void_p), ("colname", C.c_void_p),
+                ("name", C.c_char_p)]
+
+
+class SkOptions(C.Structure):
+    _fields_ = [("primal_tol", C.c_double), ("dual_tol", C.c_double), ("pivot_tol", C.c_double),
+                ("time_limit", C.c_double), ("iteration_limit", C.c_longlong),
+                ("node_limit", C.c_longlong), ("presolve", C.c_int), ("scaling", C.c_int),
+                ("refactor_interval", C.c_int), ("verbosity", C.c_int), ("threads", C.c_int),
+                ("mip_gap_abs", C.c_double), ("mip_gap_rel", C.c_double), ("mip_cuts", C.c_int),
+                ("mip_heuristics", C.c_int), ("dual_simplex", C.c_int), ("lp_engine", C.c_int),
+                ("random_seed", C.c_ulonglong)]
+
+
+class SkSolution(C.Structure):
+    _fields_ = [("result", C.c_int), ("objective", C.c_double), ("x", dptr), ("y", dptr),
+                ("rc", dptr), ("rowact", dptr), ("ncol", C.c_int), ("nrow", C.c_int),
+                ("iterations", C.c_longlong), ("nodes", C.c_longlong),
+                ("solve_seconds", C.c_double), ("primal_infeasibility", C.c_double),
+                ("dual_infeasibility", C.c_double), ("complementarity", C.c_double),
+                ("mip_gap", C.c_double), ("dual_bound", C.c_double)]
+
+
+SK_LP_FIRST_ORDER = 2
+
+
+def build_sk_model(keep: _Keep, inst, quadratic=False):
+    """An sk_model view over an instance dict (A converted to CSC)."""
+    import importlib.util
+    m, n = inst["m"], inst["n"]
+    if "csc" not in inst:
+        rows = np.repeat(np.arange(m, dtype=np.int32), np.diff(inst["ptr"]))
+        order = np.argsort(inst["idx"], kind="stable")
+        cp = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(np.bincount(inst["idx"], minlength=n), out=cp[1:])
+        inst["csc"] = (cp.astype(np.int32), rows[order].astype(np.int32), inst["val"][order].copy())
+    cp, ci, cx = inst["csc"]
+    model = SkModel()
+    model.nrow, model.ncol = m, n
+    nnz = int(cp[-1])
+    model.A = SkCsc(m, n, _p(keep.i(cp), iptr), _p(keep.i(ci), iptr), _p(keep.d(cx)), max(nnz, 1))
+    if quadratic and "q_ptr" in inst:
+        q = SkCsc(n, n, _p(keep.i(inst["q_ptr"]), iptr), _p(keep.i(inst["q_idx"]), iptr),
+                  _p(keep.d(inst["q_val"])), max(int(inst["q_ptr"][-1]), 1))
+        keep.refs.append(q)
+        model.Q = C.pointer(q)
+    for k, f in (("c", "c"), ("rl", "rlow"), ("ru", "rupp"), ("cl", "clow"), ("cu", "cupp")):
+        setattr(model, f, _p(keep.d(inst[k])))
+    vt = np.zeros(max(n, 1), dtype=np.uint8)
+    keep.refs.append(vt)
+    model.vartype = vt.ctypes.data_as(C.POINTER(C.c_ubyte))
+    model.objshift = 0.0
+    model.objsense = 1.0
+    return model
+
+
+def ref_options(primal_tol=1e-7, dual_tol=1e-7, iteration_limit=0, time_limit=0.0,
+                lp_engine=SK_LP_FIRST_ORDER, threads=1):
+    lib = load("ref")
+    o = SkOptions()
+    lib.sk_options_default(C.byref(o))
+    o.primal_tol, o.dual_tol = primal_tol, dual_tol
+    o.iteration_limit, o.time_limit = iteration_limit, time_limit
+    o.lp_engine, o.threads, o.verbosity = lp_engine, threads, 0
+    return o
+
+
+def ref_sk_solve(inst, quadratic=False, **opts):
+    """Runs the reference's sk_solve; returns (status, dict with x, y, rowact, fields)."""
+    lib = load("ref")
+    keep = _Keep()
+    model = build_sk_model(keep, inst, quadratic)
+    o = ref_options(**opts)
+    s = SkSolution()
+    lib.sk_solution_init(C.byref(s))
+    st = lib.sk_solve(C.byref(model), C.byref(o), C.byref(s))
+    out = {k: getattr(s, k) for k, _ in SkSolution._fields_ if k not in ("x", "y", "rc", "rowact")}
+    n, m = inst["n"], inst["m"]
+    out["x"] = np.ctypeslib.as_array(s.x, (n,)).copy() if s.x and n else np.zeros(n)
+    out["y"] = np.ctypeslib.as_array(s.y, (m,)).copy() if s.y and m else np.zeros(m)
+    out["rowact"] = np.ctypeslib.as_array(s.rowact, (m,)).copy() if s.rowact and m else np.zeros(m)
+    lib.sk_solution_free(C.byref(s))
+    return st, out
+
+
+def ref_sk_verify(inst, x, y, quadratic=False):
+    lib = load("ref")
+    keep = _Keep()
+    model = build_sk_model(keep, inst, quadratic)
+    s = SkSolution()
+    lib.sk_solution_init(C.byref(s))
+    xs = keep.d(x)
+    s.x = _p(xs)
+    if y is not None:
+        s.y = _p(keep.d(y))
+    st = lib.sk_verify(C.byref(model), C.byref(s))
+    return st, {"objective": s.objective, "primal_infeasibility": s.primal_infeasibility,
+                "dual_infeasibility": s.dual_infeasibility, "complementarity": s.complementarity}
+
+
+def ref_sk_scale_model(inst, passes=4):
+    lib = load("ref")
+    keep = _Keep()
+    model = build_sk_model(keep, inst)
+    r, c = np.zeros(inst["m"]), np.zeros(inst["n"])
+    lib.sk_scale_model(C.byref(model), _p(r), _p(c), C.c_int(passes))
+    return r, c

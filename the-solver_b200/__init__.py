@@ -1,0 +1,297 @@
+"""Python view of the B200 PDHG engine's C ABI (lib/libsankhya_cuda.so).
+
+The engine itself is C++/CUDA behind the reference's C entry points; this
+module only loads the shared library with ctypes and marshals numpy arrays,
+for tests and benchmarks. It raises when the library is missing: there is no
+Python or CPU fallback.
+
+Import it by path (the folder name is not a Python identifier):
+    spec = importlib.util.spec_from_file_location("sankhya_b200", "<repo>/the-solver_b200/__init__.py")
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libsankhya_cuda.so")
+
+dptr = C.POINTER(C.c_double)
+iptr = C.POINTER(C.c_int)
+
+# Every symbol declared in include/sankhya_cuda.h and include/sankhya_b200.h.
+REFERENCE_SYMBOLS = (
+    "sankhya_cuda_csr_create", "sankhya_cuda_csr_destroy", "sankhya_cuda_spmv_device_f64",
+    "sankhya_cuda_spmv_transpose_device_f64", "sankhya_cuda_axpy_device_f64", "sankhya_cuda_lp_pdhg",
+    "sankhya_cuda_qp_pdhg_preconditioned_with_dual", "sankhya_cuda_diagonal_qp_pdhg",
+    "sankhya_cuda_sparse_qp_pdhg", "sankhya_cuda_qp_pdhg_preconditioned", "sankhya_cuda_spmv_f64",
+    "sankhya_cuda_axpy_f64", "sankhya_cuda_last_error",
+)
+EXTENSION_SYMBOLS = (
+    "sankhya_b200_set_timing", "sankhya_b200_last_timing", "sankhya_b200_pdhg_loop",
+    "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve",
+)
+
+_lib = None
+
+
+def build(verbose: bool = False) -> str:
+    """Compiles lib/libsankhya_cuda.so for sm_100a with nvcc (make)."""
+    out = subprocess.run(["make", "-C", HERE, "-j8"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("building libsankhya_cuda.so failed:\n" + out.stdout + out.stderr)
+    if verbose:
+        print(out.stdout)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {HERE}`")
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+class CSR(C.Structure):
+    """SankhyaCudaCSR."""
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("nnz", C.c_int),
+                ("device_row_offsets", C.c_void_p), ("device_column_indices", C.c_void_p),
+                ("device_values", C.c_void_p)]
+
+
+class Settings(C.Structure):
+    """SankhyaCudaLPSettings."""
+    _fields_ = [("max_iterations", C.c_int), ("check_every", C.c_int), ("tau", C.c_double),
+                ("sigma", C.c_double), ("theta", C.c_double), ("tolerance", C.c_double),
+                ("time_limit", C.c_double)]
+
+
+class Result(C.Structure):
+    """SankhyaCudaLPResult."""
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("objective", C.c_double),
+                ("maximum_row_violation", C.c_double), ("maximum_step", C.c_double),
+                ("maximum_kkt_residual", C.c_double), ("maximum_dual_residual", C.c_double),
+                ("maximum_complementarity", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Timing(C.Structure):
+    """SankhyaB200Timing."""
+    _fields_ = [("iterations", C.c_int), ("checkpoints", C.c_int), ("kernel_launches", C.c_int),
+                ("per_kernel_samples", C.c_int), ("loop_ms", C.c_double), ("checkpoint_ms", C.c_double),
+                ("dual_kernel_ms", C.c_double), ("primal_kernel_ms", C.c_double), ("h2d_ms", C.c_double),
+                ("d2h_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LoopResult(C.Structure):
+    """SankhyaB200LoopResult."""
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("numeric_failure", C.c_int),
+                ("dual_step", C.c_double), ("anorm", C.c_double), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PdlpSettings(C.Structure):
+    """SankhyaB200PdlpSettings."""
+    _fields_ = [("struct_version", C.c_int), ("max_iterations", C.c_int), ("restart_period", C.c_int),
+                ("power_iterations", C.c_int), ("adaptive_step", C.c_int), ("scaling", C.c_int),
+                ("ruiz_iterations", C.c_int), ("precision", C.c_int), ("eps_optimal", C.c_double),
+                ("time_limit", C.c_double), ("eta_min_factor", C.c_double), ("eta_max_factor", C.c_double),
+                ("ruiz_tolerance", C.c_double)]
+
+
+class PdlpResult(C.Structure):
+    """SankhyaB200PdlpResult."""
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("restarts", C.c_int),
+                ("rejected_steps", C.c_int), ("host_syncs", C.c_int), ("refinements", C.c_int),
+                ("primal_objective", C.c_double), ("dual_objective", C.c_double),
+                ("relative_primal_residual", C.c_double), ("relative_dual_residual", C.c_double),
+                ("relative_gap", C.c_double), ("matrix_norm", C.c_double), ("final_step_size", C.c_double),
+                ("primal_weight", C.c_double), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+SCALE_RUIZ, SCALE_POCK_CHAMBOLLE, SCALE_POW2 = 1, 2, 4
+FP64, FP32_REFINE = 0, 1
+
+
+def _declare(L):
+    P = C.POINTER
+    L.sankhya_cuda_csr_create.argtypes = [P(CSR), C.c_int, C.c_int, C.c_int, iptr, iptr, dptr]
+    L.sankhya_cuda_csr_destroy.argtypes = [P(CSR)]
+    L.sankhya_cuda_csr_destroy.restype = None
+    L.sankhya_cuda_last_error.restype = C.c_char_p
+    L.sankhya_cuda_spmv_device_f64.argtypes = [P(CSR), C.c_void_p, C.c_void_p]
+    L.sankhya_cuda_spmv_transpose_device_f64.argtypes = [P(CSR), C.c_void_p, C.c_void_p]
+    L.sankhya_cuda_axpy_device_f64.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+    L.sankhya_cuda_spmv_f64.argtypes = [C.c_int, C.c_int, C.c_int, iptr, iptr, dptr, dptr, dptr]
+    L.sankhya_cuda_axpy_f64.argtypes = [C.c_int, C.c_double, dptr, dptr]
+    L.sankhya_cuda_lp_pdhg.argtypes = [P(CSR), dptr, dptr, dptr, dptr, dptr, Settings, dptr, P(Result)]
+    L.sankhya_cuda_diagonal_qp_pdhg.argtypes = [P(CSR), dptr, dptr, dptr, dptr, dptr, dptr, Settings, dptr,
+                                                P(Result)]
+    L.sankhya_cuda_sparse_qp_pdhg.argtypes = [P(CSR), P(CSR), dptr, dptr, dptr, dptr, dptr, Settings, dptr,
+                                              P(Result)]
+    L.sankhya_cuda_qp_pdhg_preconditioned.argtypes = [P(CSR), P(CSR), dptr, dptr, dptr, dptr, dptr, dptr, dptr,
+                                                      dptr, Settings, dptr, P(Result)]
+    L.sankhya_cuda_qp_pdhg_preconditioned_with_dual.argtypes = [P(CSR), P(CSR), dptr, dptr, dptr, dptr, dptr,
+                                                                dptr, dptr, dptr, Settings, dptr, dptr,
+                                                                P(Result)]
+    L.sankhya_b200_set_timing.argtypes = [C.c_int]
+    L.sankhya_b200_set_timing.restype = None
+    L.sankhya_b200_last_timing.argtypes = [P(Timing)]
+    L.sankhya_b200_last_timing.restype = None
+    L.sankhya_b200_pdhg_loop.argtypes = [C.c_void_p, C.c_void_p, dptr, dptr, dptr, P(LoopResult)]
+    if hasattr(L, "sankhya_b200_pdlp_solve"):
+        L.sankhya_b200_pdlp_default_settings.argtypes = [P(PdlpSettings)]
+        L.sankhya_b200_pdlp_default_settings.restype = None
+        L.sankhya_b200_pdlp_solve.argtypes = [P(CSR), dptr, dptr, dptr, dptr, dptr, P(PdlpSettings), dptr,
+                                              dptr, dptr, dptr, P(PdlpResult)]
+
+
+def _d(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(dptr)
+
+
+def last_error() -> str:
+    return lib().sankhya_cuda_last_error().decode()
+
+
+class Matrix:
+    """A device-resident CSR made by sankhya_cuda_csr_create."""
+
+    def __init__(self, rows, cols, ptr, idx, val):
+        self.ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+        self.idx = np.ascontiguousarray(idx, dtype=np.int32)
+        self.val = np.ascontiguousarray(val, dtype=np.float64)
+        self.handle = CSR()
+        rc = lib().sankhya_cuda_csr_create(C.byref(self.handle), int(rows), int(cols), int(self.val.shape[0]),
+                                           self.ptr.ctypes.data_as(iptr), self.idx.ctypes.data_as(iptr),
+                                           self.val.ctypes.data_as(dptr))
+        if rc != 0:
+            raise RuntimeError(f"sankhya_cuda_csr_create failed: {last_error()}")
+
+    @classmethod
+    def from_instance(cls, inst, hessian=False):
+        if hessian:
+            return cls(inst["n"], inst["n"], inst["q_ptr"], inst["q_idx"], inst["q_val"])
+        return cls(inst["m"], inst["n"], inst["ptr"], inst["idx"], inst["val"])
+
+    def close(self):
+        if self.handle is not None:
+            lib().sankhya_cuda_csr_destroy(C.byref(self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def settings(max_iterations=1000, check_every=10, tau=0.0, sigma=0.0, theta=1.0, tolerance=1e-6,
+             time_limit=0.0) -> Settings:
+    return Settings(max_iterations, check_every, tau, sigma, theta, tolerance, time_limit)
+
+
+def pdhg(matrix: Matrix, inst, s: Settings, hessian: Matrix | None = None, qdiag=None, primal_steps=None,
+         dual_steps=None, want_dual=False, entry: str | None = None, **over):
+    """Calls one of the five *_pdhg entry points; returns (rc, x, y, result)."""
+    L = lib()
+    get = lambda k: _d(over[k]) if k in over else _d(inst[k])
+    c, rl, ru, cl, cu = get("c"), get("rl"), get("ru"), get("cl"), get("cu")
+    n, m = matrix.handle.cols, matrix.handle.rows
+    x = np.zeros(n)
+    y = np.zeros(m) if want_dual else None
+    res = Result()
+    qd, ps, ds = _d(qdiag), _d(primal_steps), _d(dual_steps)
+    h = C.byref(hessian.handle) if hessian is not None else None
+    if entry is None:
+        if ps is not None:
+            entry = "with_dual" if want_dual else "preconditioned"
+        elif hessian is not None:
+            entry = "sparse"
+        elif qd is not None:
+            entry = "diagonal"
+        else:
+            entry = "lp"
+    M = C.byref(matrix.handle)
+    if entry == "lp":
+        rc = L.sankhya_cuda_lp_pdhg(M, _p(c), _p(rl), _p(ru), _p(cl), _p(cu), s, _p(x), C.byref(res))
+    elif entry == "diagonal":
+        rc = L.sankhya_cuda_diagonal_qp_pdhg(M, _p(qd), _p(c), _p(rl), _p(ru), _p(cl), _p(cu), s, _p(x),
+                                             C.byref(res))
+    elif entry == "sparse":
+        rc = L.sankhya_cuda_sparse_qp_pdhg(M, h, _p(c), _p(rl), _p(ru), _p(cl), _p(cu), s, _p(x), C.byref(res))
+    elif entry == "preconditioned":
+        rc = L.sankhya_cuda_qp_pdhg_preconditioned(M, h, _p(qd), _p(c), _p(rl), _p(ru), _p(cl), _p(cu), _p(ps),
+                                                   _p(ds), s, _p(x), C.byref(res))
+    elif entry == "with_dual":
+        rc = L.sankhya_cuda_qp_pdhg_preconditioned_with_dual(M, h, _p(qd), _p(c), _p(rl), _p(ru), _p(cl), _p(cu),
+                                                             _p(ps), _p(ds), s, _p(x), _p(y), C.byref(res))
+    else:
+        raise ValueError(entry)
+    return rc, x, y, res.as_dict()
+
+
+def set_timing(level: int):
+    lib().sankhya_b200_set_timing(int(level))
+
+
+def last_timing() -> dict:
+    t = Timing()
+    lib().sankhya_b200_last_timing(C.byref(t))
+    return t.as_dict()
+
+
+def spmv_host(rows, cols, ptr, idx, val, x):
+    y = np.zeros(rows)
+    ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    val, x = _d(val), _d(x)
+    rc = lib().sankhya_cuda_spmv_f64(rows, cols, int(val.shape[0]), ptr.ctypes.data_as(iptr),
+                                     idx.ctypes.data_as(iptr), _p(val), _p(x), _p(y))
+    return rc, y
+
+
+def axpy_host(alpha, x, y):
+    x, y = _d(x), _d(y).copy()
+    rc = lib().sankhya_cuda_axpy_f64(int(x.shape[0]), float(alpha), _p(x), _p(y))
+    return rc, y
+
+
+def pdlp_default_settings() -> PdlpSettings:
+    s = PdlpSettings()
+    lib().sankhya_b200_pdlp_default_settings(C.byref(s))
+    return s
+
+
+def pdlp_solve(matrix: Matrix, inst, s: PdlpSettings | None = None, x0=None, y0=None, want_dual=True, **over):
+    L = lib()
+    s = s or pdlp_default_settings()
+    get = lambda k: _d(over[k]) if k in over else _d(inst[k])
+    c, rl, ru, cl, cu = get("c"), get("rl"), get("ru"), get("cl"), get("cu")
+    n, m = matrix.handle.cols, matrix.handle.rows
+    x = np.zeros(n)
+    y = np.zeros(m) if want_dual else None
+    res = PdlpResult()
+    rc = L.sankhya_b200_pdlp_solve(C.byref(matrix.handle), _p(c), _p(rl), _p(ru), _p(cl), _p(cu), C.byref(s),
+                                   _p(_d(x0)), _p(_d(y0)), _p(x), _p(y), C.byref(res))
+    return rc, x, y, res.as_dict()

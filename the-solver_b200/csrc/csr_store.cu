@@ -1,0 +1,305 @@
+// Device CSR store: validation + upload (sankhya_cuda_csr_create/destroy), the
+// private transpose and row-tile schedule kept beside each matrix, the
+// thread-local error text, the engine stream and launch sizing.
+//
+// Reference behaviour followed: cuda/src/sankhya_cuda.cu:10-21 (error text),
+// :116-152 (validation order and messages, destroy-before-create, zeroed
+// handle on failure), :154-163 (destroy).
+#include "engine.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <unordered_map>
+
+namespace b200 {
+
+namespace {
+thread_local char g_last_error[512] = "";
+}
+
+int fail_msg(const char* message) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s", message);
+    return -1;
+}
+
+int fail_cuda(const char* operation, cudaError_t error) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s", operation, cudaGetErrorString(error));
+    return -1;
+}
+
+void clear_error() { g_last_error[0] = '\0'; }
+
+// ------------------------------------------------------------------ tiles
+
+std::vector<int> build_tiles(int rows, const int* ptr) {
+    std::vector<int> tiles;
+    tiles.reserve(static_cast<size_t>(rows) / 64 + 2);
+    int r = 0;
+    while (r < rows) {
+        tiles.push_back(r);
+        const int len = ptr[r + 1] - ptr[r];
+        if (len > kTileNnz) {
+            ++r;
+            continue;
+        }
+        const int start = r;
+        int nnz = 0;
+        while (r < rows && r - start < kMaxTileRows) {
+            const int l = ptr[r + 1] - ptr[r];
+            if (nnz + l > kTileNnz) break;
+            nnz += l;
+            ++r;
+        }
+    }
+    tiles.push_back(rows);
+    return tiles;
+}
+
+// ------------------------------------------------------------------ plans
+
+Plan::~Plan() {
+    int current = -1;
+    cudaGetDevice(&current);
+    if (current != device) cudaSetDevice(device);
+    cudaFree(d_tile_a);
+    cudaFree(d_at_ptr);
+    cudaFree(d_at_idx);
+    cudaFree(d_at_val);
+    cudaFree(d_tile_at);
+    for (void* p : workspace) cudaFree(p);
+    if (current >= 0 && current != device) cudaSetDevice(current);
+}
+
+static int upload(void** dst, const void* src, size_t bytes, const char* what) {
+    if (bytes == 0) { *dst = nullptr; return 0; }
+    cudaError_t e = cudaMalloc(dst, bytes);
+    if (e != cudaSuccess) { *dst = nullptr; return fail_cuda(what, e); }
+    e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail_cuda(what, e);
+    return 0;
+}
+
+int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const double* h_val,
+              std::shared_ptr<Plan>* out) {
+    auto plan = std::make_shared<Plan>();
+    cudaGetDevice(&plan->device);
+    const int rows = m->rows, cols = m->cols, nnz = m->nnz;
+
+    std::vector<int> tiles_a = build_tiles(rows, h_ptr);
+    // Transpose by counting sort: rows of A visited in order, so each column
+    // of A (row of A^T) lists its row indices ascending.
+    std::vector<int> at_ptr(static_cast<size_t>(cols) + 1, 0);
+    std::vector<int> at_idx(static_cast<size_t>(nnz));
+    std::vector<double> at_val(static_cast<size_t>(nnz));
+    for (int p = 0; p < nnz; ++p) at_ptr[static_cast<size_t>(h_idx[p]) + 1]++;
+    for (int j = 0; j < cols; ++j) at_ptr[j + 1] += at_ptr[j];
+    {
+        std::vector<int> next(at_ptr.begin(), at_ptr.end() - 1);
+        for (int r = 0; r < rows; ++r)
+            for (int p = h_ptr[r]; p < h_ptr[r + 1]; ++p) {
+                const int slot = next[h_idx[p]]++;
+                at_idx[slot] = r;
+                at_val[slot] = h_val[p];
+            }
+    }
+    std::vector<int> tiles_at = build_tiles(cols, at_ptr.data());
+
+    if (upload(reinterpret_cast<void**>(&plan->d_tile_a), tiles_a.data(), tiles_a.size() * sizeof(int), "cudaMalloc tiles(A)") ||
+        upload(reinterpret_cast<void**>(&plan->d_at_ptr), at_ptr.data(), at_ptr.size() * sizeof(int), "cudaMalloc A^T offsets") ||
+        upload(reinterpret_cast<void**>(&plan->d_at_idx), at_idx.data(), at_idx.size() * sizeof(int), "cudaMalloc A^T indices") ||
+        upload(reinterpret_cast<void**>(&plan->d_at_val), at_val.data(), at_val.size() * sizeof(double), "cudaMalloc A^T values") ||
+        upload(reinterpret_cast<void**>(&plan->d_tile_at), tiles_at.data(), tiles_at.size() * sizeof(int), "cudaMalloc tiles(A^T)"))
+        return -1;
+
+    plan->a.rows = rows;
+    plan->a.cols = cols;
+    plan->a.nnz = nnz;
+    plan->a.ptr = static_cast<const int*>(m->device_row_offsets);
+    plan->a.idx = static_cast<const int*>(m->device_column_indices);
+    plan->a.val = static_cast<const double*>(m->device_values);
+    plan->a.ntiles = static_cast<int>(tiles_a.size()) - 1;
+    plan->a.tile_row = plan->d_tile_a;
+    plan->at.rows = cols;
+    plan->at.cols = rows;
+    plan->at.nnz = nnz;
+    plan->at.ptr = plan->d_at_ptr;
+    plan->at.idx = plan->d_at_idx;
+    plan->at.val = plan->d_at_val;
+    plan->at.ntiles = static_cast<int>(tiles_at.size()) - 1;
+    plan->at.tile_row = plan->d_tile_at;
+    *out = std::move(plan);
+    return 0;
+}
+
+namespace {
+std::mutex g_registry_mutex;
+std::unordered_map<const void*, std::shared_ptr<Plan>>& registry() {
+    static auto* map = new std::unordered_map<const void*, std::shared_ptr<Plan>>();
+    return *map;
+}
+}  // namespace
+
+void register_plan(const void* key, std::shared_ptr<Plan> plan) {
+    std::lock_guard<std::mutex> lock(g_registry_mutex);
+    registry()[key] = std::move(plan);
+}
+
+void unregister_plan(const void* key) {
+    std::shared_ptr<Plan> doomed;
+    {
+        std::lock_guard<std::mutex> lock(g_registry_mutex);
+        auto it = registry().find(key);
+        if (it == registry().end()) return;
+        doomed = std::move(it->second);
+        registry().erase(it);
+    }
+}
+
+int get_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out) {
+    if (m == nullptr) return fail_msg("null device CSR pointer");
+    {
+        std::lock_guard<std::mutex> lock(g_registry_mutex);
+        auto it = registry().find(m->device_row_offsets);
+        if (it != registry().end() && it->second->a.rows == m->rows && it->second->a.cols == m->cols &&
+            it->second->a.nnz == m->nnz && it->second->a.val == m->device_values &&
+            it->second->a.idx == m->device_column_indices) {
+            *out = it->second;
+            return 0;
+        }
+    }
+    // A handle filled by the caller: bring its CSR back once and plan it.
+    if (m->rows < 0 || m->cols < 0 || m->nnz < 0) return fail_msg("invalid device CSR dimensions");
+    if (m->device_row_offsets == nullptr || (m->nnz > 0 && (m->device_column_indices == nullptr || m->device_values == nullptr)))
+        return fail_msg("null device CSR pointer");
+    std::vector<int> ptr(static_cast<size_t>(m->rows) + 1);
+    std::vector<int> idx(static_cast<size_t>(m->nnz));
+    std::vector<double> val(static_cast<size_t>(m->nnz));
+    B200_TRY(cudaMemcpy(ptr.data(), m->device_row_offsets, ptr.size() * sizeof(int), cudaMemcpyDeviceToHost), "read CSR offsets");
+    if (m->nnz > 0) {
+        B200_TRY(cudaMemcpy(idx.data(), m->device_column_indices, idx.size() * sizeof(int), cudaMemcpyDeviceToHost), "read CSR indices");
+        B200_TRY(cudaMemcpy(val.data(), m->device_values, val.size() * sizeof(double), cudaMemcpyDeviceToHost), "read CSR values");
+    }
+    if (ptr[0] != 0 || ptr[static_cast<size_t>(m->rows)] != m->nnz) return fail_msg("invalid CSR row-offset endpoints");
+    for (int r = 0; r < m->rows; ++r)
+        if (ptr[r] < 0 || ptr[r] > ptr[r + 1] || ptr[r + 1] > m->nnz) return fail_msg("invalid CSR row-offset ordering");
+    for (int p = 0; p < m->nnz; ++p)
+        if (idx[p] < 0 || idx[p] >= m->cols) return fail_msg("invalid CSR column index or coefficient");
+    return make_plan(m, ptr.data(), idx.data(), val.data(), out);
+}
+
+// ------------------------------------------------------------ stream, grid
+
+cudaStream_t engine_stream() {
+    struct PerThread {
+        cudaStream_t streams[64] = {};
+        ~PerThread() {
+            for (cudaStream_t s : streams)
+                if (s) cudaStreamDestroy(s);
+        }
+    };
+    thread_local PerThread state;
+    int device = 0;
+    cudaGetDevice(&device);
+    if (device < 0 || device >= 64) return nullptr;
+    if (!state.streams[device]) cudaStreamCreateWithFlags(&state.streams[device], cudaStreamNonBlocking);
+    return state.streams[device];
+}
+
+int grid_for(const void* kernel, int ntiles) {
+    struct Entry { const void* k; int device; int blocks; };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
+    int device = 0;
+    cudaGetDevice(&device);
+    int resident = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (const Entry& e : cache)
+            if (e.k == kernel && e.device == device) resident = e.blocks;
+        if (resident == 0) {
+            int per_sm = 0, sms = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+            resident = std::max(1, per_sm) * std::max(1, sms);
+            cache.push_back({kernel, device, resident});
+        }
+    }
+    return std::max(1, std::min(ntiles, resident));
+}
+
+TimingState& timing() {
+    thread_local TimingState state;
+    return state;
+}
+
+// ------------------------------------------------------------ small kernels
+
+__global__ void k_fill(double* __restrict__ out, double value, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += blockDim.x * gridDim.x) out[i] = value;
+}
+
+__global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += blockDim.x * gridDim.x) dst[i] = src[i];
+}
+
+}  // namespace b200
+
+using namespace b200;
+
+extern "C" const char* sankhya_cuda_last_error(void) { return g_last_error; }
+
+extern "C" void sankhya_b200_set_timing(int level) { timing().level = level; }
+
+extern "C" void sankhya_b200_last_timing(SankhyaB200Timing* out) {
+    if (out) *out = timing().last;
+}
+
+extern "C" void sankhya_cuda_csr_destroy(SankhyaCudaCSR* matrix) {
+    if (matrix == nullptr) return;
+    if (matrix->device_row_offsets) unregister_plan(matrix->device_row_offsets);
+    cudaFree(matrix->device_row_offsets);
+    cudaFree(matrix->device_column_indices);
+    cudaFree(matrix->device_values);
+    matrix->rows = matrix->cols = matrix->nnz = 0;
+    matrix->device_row_offsets = nullptr;
+    matrix->device_column_indices = nullptr;
+    matrix->device_values = nullptr;
+}
+
+extern "C" int sankhya_cuda_csr_create(SankhyaCudaCSR* matrix, int rows, int cols, int nnz,
+                                       const int* row_offsets, const int* column_indices,
+                                       const double* values) {
+    clear_error();
+    if (matrix == nullptr || row_offsets == nullptr || rows < 0 || cols < 0 || nnz < 0 ||
+        (nnz > 0 && (column_indices == nullptr || values == nullptr)))
+        return fail_msg("invalid persistent CSR input");
+    if (row_offsets[0] != 0 || row_offsets[rows] != nnz) return fail_msg("invalid CSR row-offset endpoints");
+    for (int r = 0; r < rows; ++r)
+        if (row_offsets[r] < 0 || row_offsets[r] > row_offsets[r + 1] || row_offsets[r + 1] > nnz)
+            return fail_msg("invalid CSR row-offset ordering");
+    for (int p = 0; p < nnz; ++p)
+        if (column_indices[p] < 0 || column_indices[p] >= cols || !std::isfinite(values[p]))
+            return fail_msg("invalid CSR column index or coefficient");
+    int devices = 0;
+    cudaError_t e = cudaGetDeviceCount(&devices);
+    if (e != cudaSuccess) return fail_cuda("cudaGetDeviceCount", e);
+    if (devices == 0) return fail_msg("no CUDA device available");
+    sankhya_cuda_csr_destroy(matrix);
+    matrix->rows = rows;
+    matrix->cols = cols;
+    matrix->nnz = nnz;
+    std::shared_ptr<Plan> plan;
+    if (upload(&matrix->device_row_offsets, row_offsets, sizeof(int) * (static_cast<size_t>(rows) + 1), "cudaMalloc row_offsets") ||
+        (nnz > 0 && upload(&matrix->device_column_indices, column_indices, sizeof(int) * static_cast<size_t>(nnz), "cudaMalloc column_indices")) ||
+        (nnz > 0 && upload(&matrix->device_values, values, sizeof(double) * static_cast<size_t>(nnz), "cudaMalloc values")) ||
+        make_plan(matrix, row_offsets, column_indices, values, &plan)) {
+        char saved[512];
+        std::snprintf(saved, sizeof(saved), "%s", g_last_error);
+        sankhya_cuda_csr_destroy(matrix);
+        fail_msg(saved);
+        return -1;
+    }
+    register_plan(matrix->device_row_offsets, std::move(plan));
+    return 0;
+}
