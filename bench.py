@@ -1,0 +1,311 @@
+#!/usr/bin/env python3
+"""Benchmark of the fused PDHG iteration on the large power-law LP.
+
+Workload (one GPU): LP with m = 1,000,000 rows, n = 2,000,000 columns and about
+20,000,000 nonzeros, column degrees Zipf(1.5) capped at 1,000, rows uniform,
+|a| log-uniform in [1e-3, 1e3] with random signs, bounds [0, 10], rows centred on
+A x0 (the-solver_b200/instances.py: lp_config1, seed 1). FP64 throughout.
+
+A step is one call of the reference C entry point sankhya_cuda_lp_pdhg with
+max_iterations = check_every = ITERS_PER_STEP: ITERS_PER_STEP fused PDHG
+iterations plus one checkpoint evaluation, host arrays in and out.
+
+  value   GB/s of algorithmic bytes, timed on the engine's stream with CUDA
+          events around the iteration kernels and checkpoints (inputs resident)
+  e2e     the same metric over host wall time of whole C-ABI calls from pinned
+          host buffers (uploads of c and bounds, solution download included)
+Algorithmic bytes of one iteration (each vector element and nonzero once):
+  A-side launch : 12 nnz + 4 (m+1) + 8 n (x_bar gather) + 32 m (y, rl, ru, y_new)
+  A'-side launch: 12 nnz + 4 (n+1) + 8 m (y_new gather) + 48 n (x, c, cl, cu, x_new, x_bar)
+
+--impl reference runs the reference's own CPU PDHG (sk_solve with
+lp_engine = SK_LP_FIRST_ORDER from its C sources, oracle/_ref) on the same
+instance and reports the same metric over its loop time.
+Multi-GPU: replicas only (one independent instance per rank, no exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+ITERS_PER_STEP = 100
+SEED = 1
+M, N, NNZ = 1_000_000, 2_000_000, 20_000_000
+WORKLOAD = "lp_config1: m=1e6, n=2e6, nnz~2e7, Zipf(1.5) columns, |a| log-U[1e-3,1e3], FP64"
+METRIC = "PDHG fused-iteration throughput (algorithmic HBM bytes), power-law LP 1Mx2M, 20M nnz"
+
+
+def _load(name, path):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dual_bytes(m, n, nnz):
+    return 12 * nnz + 4 * (m + 1) + 8 * n + 32 * m
+
+
+def primal_bytes(m, n, nnz):
+    return 12 * nnz + 4 * (n + 1) + 8 * m + 48 * n
+
+
+def iteration_bytes(m, n, nnz):
+    return dual_bytes(m, n, nnz) + primal_bytes(m, n, nnz)
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self):
+        rows = [r.split(",") for r in getattr(self, "out", "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier_max(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reference_loop_gbs(inst, iterations):
+    """The reference's sk_solve (SK_LP_FIRST_ORDER) for `iterations` iterations;
+    returns (GB/s over its loop time, loop seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    st, out = O.ref_sk_solve(inst, primal_tol=1e-300, dual_tol=1e-300, iteration_limit=iterations)
+    if st != 0:
+        raise RuntimeError(f"reference sk_solve failed with status {st}")
+    secs = out["solve_seconds"]
+    nnz = int(inst["ptr"][-1])
+    return iteration_bytes(inst["m"], inst["n"], nnz) * out["iterations"] / secs / 1e9, secs, out["iterations"]
+
+
+def cpu_baseline(inst, target_seconds=12.0):
+    """Bounded sample of the reference CPU PDHG on this instance (rank 0, N=1)."""
+    gbs1, secs1, it1 = reference_loop_gbs(inst, 1)
+    iters = int(max(2, min(200, target_seconds / max(secs1, 1e-3))))
+    gbs, secs, its = reference_loop_gbs(inst, iters)
+    return {"value": round(gbs, 4), "unit": "GB/s", "cores": 1, "kind": "reference",
+            "sample": f"{its} iterations of sk_solve (SK_LP_FIRST_ORDER, 1 thread, built from the reference's "
+                      f"c/src without OpenMP) on the same instance, {secs:.2f} s of loop time"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    inst = I.lp_config1(SEED)
+    nnz = int(inst["ptr"][-1])
+    per_step = 2  # iterations of the reference loop per step: bounded sample of the workload
+    for _ in range(args.warmup):
+        reference_loop_gbs(inst, 1)
+    total_secs, total_iters = 0.0, 0
+    for _ in range(args.steps):
+        gbs, secs, its = reference_loop_gbs(inst, per_step)
+        total_secs += secs
+        total_iters += its
+    value = iteration_bytes(M if inst["m"] == M else inst["m"], inst["n"], nnz) * total_iters / total_secs / 1e9
+    line = {"metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * total_secs / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "m": inst["m"], "n": inst["n"], "nnz": nnz,
+                       "iterations_per_step": per_step, "seed": SEED},
+            "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": 1, "kind": "reference",
+                             "sample": f"{per_step} iterations of the reference sk_solve first-order loop per step"},
+            "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_engine(args, world, rank, local):
+    import torch
+    E = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
+    I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    t0 = time.time()
+    inst = I.lp_config1(SEED + rank)
+    m, n, nnz = inst["m"], inst["n"], int(inst["ptr"][-1])
+    gen_s = time.time() - t0
+    A = E.Matrix.from_instance(inst)
+    # pinned host copies of the per-call inputs and the solution
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory().numpy()
+    host = {k: pin(inst[k]) for k in ("c", "rl", "ru", "cl", "cu")}
+    x_out = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    # steps: 0.9 / (1 + mass) per row / column (the reference CPU path's diagonal steps)
+    rows = np.repeat(np.arange(m), np.diff(inst["ptr"]))
+    rmass = np.bincount(rows, weights=np.abs(inst["val"]), minlength=m)
+    cmass = np.bincount(inst["idx"], weights=np.abs(inst["val"]), minlength=n)
+    ps, ds = pin(0.9 / (1 + cmass)), pin(0.9 / (1 + rmass))
+    s = E.settings(ITERS_PER_STEP, ITERS_PER_STEP, 0.0, 0.0, 1.0, 1e-12)
+
+    def step():
+        rc, x, y, r = E.pdhg(A, host, s, primal_steps=ps, dual_steps=ds, entry="preconditioned")
+        if rc not in (0,):
+            raise RuntimeError(f"sankhya_cuda_qp_pdhg_preconditioned returned {rc}: {E.last_error()}")
+        return r
+
+    # per-kernel durations (timing level 2: events around every launch), untimed
+    E.set_timing(2)
+    step()
+    t_kern = E.last_timing()
+    E.set_timing(1)
+    for _ in range(max(3, args.warmup)):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    dev_ms, launches, iters = 0.0, 0, 0
+    with ClockSampler(local) as clk:
+        t_start = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+            t = E.last_timing()
+            dev_ms += t["loop_ms"] + t["checkpoint_ms"]
+            launches += t["kernel_launches"]
+            iters += t["iterations"]
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t_start
+    barrier(world)
+    wall = barrier_max(wall, world)
+    dev_ms = barrier_max(dev_ms, world)
+    bytes_iter = iteration_bytes(m, n, nnz)
+    value = world * bytes_iter * iters / (dev_ms / 1e3) / 1e9
+    e2e = world * bytes_iter * iters / wall / 1e9
+    if rank != 0:
+        return 0
+    peak, peak_kind = measured_peak()
+    d_ms, p_ms = t_kern["dual_kernel_ms"], t_kern["primal_kernel_ms"]
+    dom_ms, dom_bytes, dom_name = (p_ms, primal_bytes(m, n, nnz), "A'-side (primal) launch") if p_ms >= d_ms else \
+        (d_ms, dual_bytes(m, n, nnz), "A-side (dual) launch")
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_lp_config1.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("primal" if p_ms >= d_ms else "dual")
+        except Exception:
+            traffic = None
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "m": m, "n": n, "nnz": nnz, "iterations_per_step": ITERS_PER_STEP,
+                       "seed": SEED, "entry_point": "sankhya_cuda_qp_pdhg_preconditioned (LP, diagonal steps)",
+                       "l2": f"inputs larger than L2: {(12 * nnz * 2) / 1e6:.0f} MB of A and A^T streamed per "
+                             f"iteration", "parallelism": "replicas" if world > 1 else "single"},
+            "iterations_per_s": round(world * iters / (dev_ms / 1e3), 1),
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1) if achieved else None,
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": round(dom_ms, 4),
+                         "other_launch_ms": round(d_ms if p_ms >= d_ms else p_ms, 4)},
+            "e2e": {"value": round(e2e, 2), "unit": "GB/s",
+                    "h2d_bytes_per_step": 8 * (4 * n + 3 * m), "d2h_bytes_per_step": 8 * n},
+            "gpu_launches": launches, "clocks": clk.summary(), "setup_s": {"generate": round(gen_s, 1)}}
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(inst)
+        except Exception as exc:  # the reference core is test infrastructure; report why it is missing
+            line["cpu_baseline"] = {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference",
+                                    "sample": f"unavailable: {exc}"}
+    print(json.dumps(line), flush=True)
+    A.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_engine(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

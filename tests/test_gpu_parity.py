@@ -19,12 +19,21 @@ def fixed_settings(engine, **kw):
 
 
 def run_both(engine, oracle, inst, s, **kw):
+    """Device and oracle on the same input. Entry points without a dual output
+    are compared on x and the result fields; y is compared through the
+    *_with_dual entry point (scalar steps passed as constant step vectors, which
+    is the same arithmetic)."""
     A = engine.Matrix.from_instance(inst)
     H = engine.Matrix.from_instance(inst, hessian=True) if kw.pop("hessian", False) else None
     rc, x, y, r = engine.pdhg(A, inst, engine.settings(**s), hessian=H, want_dual=True,
                               entry="with_dual" if "primal_steps" in kw else None, **kw)
-    orc_kw = dict(kw)
-    rc2, x2, y2, r2 = oracle.fixed_pdhg(inst, s, hessian=H is not None, **orc_kw)
+    rc2, x2, y2, r2 = oracle.fixed_pdhg(inst, s, hessian=H is not None, **kw)
+    if y is None and "primal_steps" not in kw:
+        ps = np.full(inst["n"], s["tau"])
+        ds = np.full(inst["m"], s["sigma"])
+        rcd, xd, y, rd = engine.pdhg(A, inst, engine.settings(**s), hessian=H, want_dual=True, entry="with_dual",
+                                     primal_steps=ps, dual_steps=ds, **kw)
+        assert rcd == rc and np.array_equal(xd, x) and rd == r
     return (rc, x, y, r), (rc2, x2, y2, r2)
 
 

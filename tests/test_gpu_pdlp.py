@@ -1,0 +1,96 @@
+"""Restarted PDLP (sankhya_b200_pdlp_solve) against the reference's PDLP tests
+(tests/lp/test_pdlp.cpp:53-206) and the oracle's restatement of GpuPdlp."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+INF = float("inf")
+
+HAND = [
+    (dict(rows=3, cols=2, dense=[1, 0, 0, 2, 3, 2], c=[-3, -5], rl=[-INF] * 3, ru=[4, 12, 18], cl=[0, 0],
+          cu=[INF, INF]), lambda x: np.allclose(x, [2, 6], atol=1e-5)),
+    (dict(rows=1, cols=2, dense=[1, 1], c=[1, 1], rl=[5], ru=[5], cl=[0, 0], cu=[10, 10]),
+     lambda x: abs(x.sum() - 5) <= 1e-6),
+    (dict(rows=1, cols=1, dense=[1], c=[-1], rl=[2], ru=[7], cl=[0], cu=[100]), lambda x: abs(x[0] - 7) <= 1e-6),
+    (dict(rows=1, cols=2, dense=[1, 1], c=[-1, -1], rl=[-INF], ru=[100], cl=[0, 0], cu=[3, 4]),
+     lambda x: np.allclose(x, [3, 4], atol=1e-6)),
+]
+
+
+def settings(engine, **kw):
+    s = engine.pdlp_default_settings()
+    s.eps_optimal = 1e-9
+    s.max_iterations = 400000
+    s.time_limit = 20.0
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+@pytest.mark.parametrize("case", range(len(HAND)))
+@pytest.mark.parametrize("scaling", [0, 3])
+def test_hand_solved_lps(engine, instances, case, scaling):
+    spec, ok = HAND[case]
+    inst = instances.small_dense_lp(**spec)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, scaling=scaling))
+    assert rc == 0 and r["status"] == 0, r
+    assert ok(x), (x, r)
+
+
+def test_fixed_step_variant(engine, instances):
+    spec, ok = HAND[0]
+    inst = instances.small_dense_lp(**spec)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, adaptive_step=0, scaling=0))
+    assert rc == 0 and r["status"] == 0 and ok(x)
+
+
+def test_sync_count_and_reproducibility(engine, instances):
+    # test_pdlp.cpp:152-206: host syncs far below iterations; bit-identical repeats
+    spec, ok = HAND[0]
+    inst = instances.small_dense_lp(**spec)
+    A = engine.Matrix.from_instance(inst)
+    s = settings(engine, scaling=0, restart_period=128)
+    runs = [engine.pdlp_solve(A, inst, s) for _ in range(3)]
+    rc, x, y, r = runs[0]
+    assert rc == 0 and r["status"] == 0
+    assert r["host_syncs"] < r["iterations"] / 8 + 16
+    for rc2, x2, y2, r2 in runs[1:]:
+        assert r2["iterations"] == r["iterations"] and np.array_equal(x2, x) and np.array_equal(y2, y)
+
+
+@pytest.mark.parametrize("name,seed,m,n,per_col", [("lp60", 12, 60, 150, 4), ("lp300", 11, 300, 700, 5)])
+def test_objective_matches_reference_simplex(engine, instances, golden_dir, name, seed, m, n, per_col):
+    ref = json.load(open(os.path.join(golden_dir, f"simplex_{name}.json")))
+    inst = instances.lp_uniform(seed, m, n, per_col)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-8))
+    assert rc == 0 and r["status"] == 0, r
+    obj = float(np.dot(inst["c"], x))
+    assert abs(obj - ref["objective"]) <= 1e-6 * (1 + abs(ref["objective"])), (obj, ref)
+
+
+def test_against_oracle_restatement(engine, oracle, instances):
+    """Unscaled PDLP: same matrix norm, same converged objective as the oracle's GpuPdlp restatement."""
+    inst = instances.lp_uniform(12, 60, 150, 4)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, scaling=0, eps_optimal=1e-8))
+    xo, yo, so = oracle.pdlp(inst, eps=1e-8, max_iterations=400000)
+    assert rc == 0 and r["status"] == 0 and so["converged"] == 1
+    assert abs(r["matrix_norm"] - so["matrix_norm"]) <= 1e-12 * so["matrix_norm"]
+    obj, objo = float(np.dot(inst["c"], x)), float(np.dot(inst["c"], xo))
+    assert abs(obj - objo) <= 1e-6 * (1 + abs(objo))
+    # same trajectory up to rounding: iteration counts agree within a few windows
+    assert abs(r["iterations"] - so["iterations"]) <= max(256, 0.2 * so["iterations"]), (r, so)
+
+
+def test_warm_start_from_solution(engine, instances):
+    inst = instances.lp_uniform(12, 60, 150, 4)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-8))
+    rc2, x2, y2, r2 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-6), x0=x, y0=y)
+    assert rc2 == 0 and r2["status"] == 0 and r2["iterations"] <= 256, r2

@@ -232,6 +232,8 @@ def pdhg(matrix: Matrix, inst, s: Settings, hessian: Matrix | None = None, qdiag
             entry = "diagonal"
         else:
             entry = "lp"
+    if entry != "with_dual":
+        y = None  # only the *_with_dual entry point returns multipliers
     M = C.byref(matrix.handle)
     if entry == "lp":
         rc = L.sankhya_cuda_lp_pdhg(M, _p(c), _p(rl), _p(ru), _p(cl), _p(cu), s, _p(x), C.byref(res))

@@ -367,7 +367,8 @@ struct Solver {
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
 
     ~Solver() {
-        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        for (auto& kv : graphs)
+            if (kv.second) cudaGraphExecDestroy(kv.second);
     }
 
     void setup_grids() {
@@ -496,6 +497,7 @@ static int solve_fixed(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessi
                        SankhyaCudaLPSettings s, const double* pstep, const double* dstep, double* solution,
                        double* dual_solution, SankhyaCudaLPResult* result) {
     clear_error();
+    (void)cudaGetLastError();  // a caller's earlier non-sticky error is not ours
     if (result == nullptr) return fail_msg("null result");
     result->status = -1;
     result->iterations = 0;
@@ -971,6 +973,7 @@ extern "C" int sankhya_b200_pdhg_loop(const sk_model* model, const sk_options* o
         return 7;
     }
     *result = SankhyaB200LoopResult{};
+    (void)cudaGetLastError();  // a caller's earlier non-sticky error is not ours
     const int rc = sk_loop(model, options, x, y, activity, result);
     return rc == 0 ? 0 : 7;
 }

@@ -1,0 +1,995 @@
+// Restarted adaptive PDLP behind sankhya_b200_pdlp_solve.
+//
+// The algorithm is the reference's GpuPdlp (src/cuda/GpuPdlp.cpp:179-534,
+// src/cuda/PdlpKernels.cu:71-518): power-iteration ||A||_2, eta = 0.9/||A||,
+// primal weight omega = ||c||/||b||, Applegate et al. adaptive step with
+// accept/reject decided on the device, restart to the better of current and
+// average at the 0.2 / 0.8 / 0.36 criteria, log-smoothed omega update,
+// relative-KKT termination. Scaling (Ruiz, Pock-Chambolle, power-of-two) is
+// computed and applied on the device.
+//
+// Per adaptive iteration three launches, all reading eta / omega / the accept
+// flag from device memory so a whole window is one CUDA graph:
+//   K1  elementwise: commit the previous candidate if accepted (x, y, sums,
+//       A x, A x_prev), then y_cand = prox(y + sigma (2 A x - A x_prev))
+//   K2  A'-side tiles: x_cand = proj(x - tau (c + A'y_cand)), block sums of |dx|^2
+//   K3  A-side tiles:  A x_cand, block sums of |dy|^2 and dy.(A dx); the last
+//       block to finish combines all partials in a fixed order and writes the
+//       new eta and the accept flag (PdlpKernels.cu:405-494).
+// The window ends with a commit, the residual sums of the current and of the
+// average iterate (PdlpKernels.cu:101-209, fused into the two products), and
+// one 200-byte copy to the host, which makes the restart decision.
+#include "engine.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <limits>
+
+namespace b200 {
+
+namespace {
+
+constexpr double kStepSafety = 0.9;
+constexpr double kMinWeight = 1e-6;
+constexpr double kMaxWeight = 1e6;
+constexpr double kSmoothing = 0.5;
+constexpr double kSufficient = 0.2;
+constexpr double kNecessary = 0.8;
+constexpr double kArtificial = 0.36;
+
+struct PdlpState {
+    double eta;
+    double omega;
+    double accepted;       // 1 when the last probe accepted its candidate
+    double updates;        // probes so far
+    double accept_count;   // accepted probes so far
+    double accepted_at_restart;
+    double eta_min, eta_max;
+    double terms_fixed;    // average divisor for the fixed-step path
+    double eta_bar, dx_sq, dy_sq, interaction;
+    unsigned int ticket;   // last-block election for the probe combine
+    unsigned int pad;
+};
+
+__device__ __forceinline__ double clampf(double v, double lo, double hi) { return fmin(fmax(v, lo), hi); }
+
+// ------------------------------------------------------------ iteration kernels
+
+// K1 (PdlpKernels.cu:499-518 commit, then :377-389 dual candidate)
+__global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, double* __restrict__ x,
+                              const double* __restrict__ x_cand, double* __restrict__ x_sum, double* __restrict__ y,
+                              double* __restrict__ y_cand, double* __restrict__ y_sum, double* __restrict__ ax,
+                              double* __restrict__ ax_prev, const double* __restrict__ ax_cand,
+                              const double* __restrict__ rl, const double* __restrict__ ru, int make_candidate) {
+    const bool acc = st->accepted != 0.0;
+    const double sigma = st->eta * st->omega;
+    const int stride = blockDim.x * gridDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        double yi = y[i], axi = ax[i], axp = ax_prev[i];
+        if (acc) {
+            const double yc = y_cand[i];
+            yi = yc;
+            y[i] = yc;
+            y_sum[i] += yc;
+            axp = axi;
+            axi = ax_cand[i];
+            ax_prev[i] = axp;
+            ax[i] = axi;
+        }
+        if (make_candidate) {
+            const double v = yi + sigma * (2.0 * axi - axp);
+            y_cand[i] = v - sigma * clampf(v / sigma, rl[i], ru[i]);
+        }
+    }
+    if (acc) {
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+            const double xc = x_cand[j];
+            x[j] = xc;
+            x_sum[j] += xc;
+        }
+    }
+}
+
+// K2 (PdlpKernels.cu:391-400 primal candidate + the |dx|^2 part of :405-430)
+struct PrimalCandEpi {
+    const PdlpState* st;
+    const double* __restrict__ x;
+    const double* __restrict__ c;
+    const double* __restrict__ cl;
+    const double* __restrict__ cu;
+    double* __restrict__ x_cand;
+    double* __restrict__ partial;
+    using Acc = Slots<1, 1u>;
+    __device__ __forceinline__ void row(int j, double aty, Acc& acc) const {
+        const double tau = st->eta / st->omega;
+        const double xj = x[j];
+        const double xc = clampf(xj - tau * (c[j] + aty), cl[j], cu[j]);
+        x_cand[j] = xc;
+        const double dx = xc - xj;
+        acc.add(0, dx * dx);
+    }
+    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
+};
+
+// K3 (A x_cand, |dy|^2, dy.(A x_cand - A x), then PdlpKernels.cu:460-494 in the last block)
+struct ProbeEpi {
+    PdlpState* st;
+    const double* __restrict__ y;
+    const double* __restrict__ y_cand;
+    const double* __restrict__ ax;
+    double* __restrict__ ax_cand;
+    double* __restrict__ partial;        // this kernel's [gridDim.x * 2]
+    const double* __restrict__ partial_dx;  // K2's [grid_dx]
+    int grid_dx;
+    using Acc = Slots<2, 3u>;
+    __device__ __forceinline__ void row(int i, double axc, Acc& acc) const {
+        ax_cand[i] = axc;
+        const double dy = y_cand[i] - y[i];
+        acc.add(0, dy * dy);
+        acc.add(1, dy * (axc - ax[i]));
+    }
+    __device__ void finish(Acc& acc, double* smem) const {
+        block_store(acc, partial, smem);
+        __shared__ bool last;
+        if (threadIdx.x == 0) {
+            __threadfence();
+            const unsigned int t = atomicAdd(&st->ticket, 1u);
+            last = (t == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (!last) return;
+        __threadfence();
+        // fixed-order combine: thread k sums a strided slice, then a fixed tree
+        __shared__ double red[3][kThreads];
+        double a = 0.0, b = 0.0, d = 0.0;
+        for (int g = threadIdx.x; g < grid_dx; g += kThreads) a += __ldcg(partial_dx + g);
+        for (int g = threadIdx.x; g < static_cast<int>(gridDim.x); g += kThreads) {
+            b += __ldcg(partial + 2 * g);
+            d += __ldcg(partial + 2 * g + 1);
+        }
+        red[0][threadIdx.x] = a;
+        red[1][threadIdx.x] = b;
+        red[2][threadIdx.x] = d;
+        __syncthreads();
+        for (int s = kThreads / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) {
+                red[0][threadIdx.x] += red[0][threadIdx.x + s];
+                red[1][threadIdx.x] += red[1][threadIdx.x + s];
+                red[2][threadIdx.x] += red[2][threadIdx.x + s];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x != 0) return;
+        const double dx_sq = red[0][0], dy_sq = red[1][0], inter = fabs(red[2][0]);
+        const double omega = st->omega;
+        const double movement = 0.5 * (omega * dx_sq + dy_sq / omega);
+        const double eta_used = st->eta;
+        const double eta_bar = (inter > 0.0 && movement > 0.0) ? movement / inter : st->eta_max;
+        const bool accept = eta_used <= eta_bar;
+        const double k = st->updates + 1.0;
+        const double shrink = 1.0 - pow(k + 1.0, -0.3);
+        const double grow = 1.0 + pow(k + 1.0, -0.6);
+        double eta_next = fmin(shrink * eta_bar, grow * eta_used);
+        if (!(eta_next > 0.0) || !isfinite(eta_next)) eta_next = eta_used;
+        eta_next = fmin(fmax(eta_next, st->eta_min), st->eta_max);
+        st->eta = eta_next;
+        st->eta_bar = eta_bar;
+        st->dx_sq = dx_sq;
+        st->dy_sq = dy_sq;
+        st->interaction = inter;
+        st->accepted = accept ? 1.0 : 0.0;
+        st->updates = k;
+        if (accept) st->accept_count += 1.0;
+        st->ticket = 0u;
+    }
+};
+
+// Fixed-step path (PdlpKernels.cu:71-97): dual on A x_bar, primal on A'y, with sums.
+struct DualFixedEpi {
+    const PdlpState* st;
+    double* __restrict__ y;
+    double* __restrict__ y_sum;
+    const double* __restrict__ rl;
+    const double* __restrict__ ru;
+    double sigma;
+    using Acc = NoAcc;
+    __device__ __forceinline__ void row(int i, double axb, Acc&) const {
+        const double v = y[i] + sigma * axb;
+        const double yi = v - sigma * clampf(v / sigma, rl[i], ru[i]);
+        y[i] = yi;
+        y_sum[i] += yi;
+    }
+    __device__ __forceinline__ void finish(Acc&, double*) const {}
+};
+
+struct PrimalFixedEpi {
+    double* __restrict__ x;
+    double* __restrict__ x_bar;
+    double* __restrict__ x_sum;
+    const double* __restrict__ c;
+    const double* __restrict__ cl;
+    const double* __restrict__ cu;
+    double tau;
+    using Acc = NoAcc;
+    __device__ __forceinline__ void row(int j, double aty, Acc&) const {
+        const double xj = x[j];
+        const double xn = clampf(xj - tau * (c[j] + aty), cl[j], cu[j]);
+        x_bar[j] = 2.0 * xn - xj;
+        x[j] = xn;
+        x_sum[j] += xn;
+    }
+    __device__ __forceinline__ void finish(Acc&, double*) const {}
+};
+
+// ----------------------------------------------------------- residual kernels
+// PdlpKernels.cu:101-209 split over the two products. Row slots (sums):
+// 0 |Ax - proj(Ax)|^2, 1 |y|^2, 2 |y - y_restart|^2, 3 -support(y).
+struct ResRowsEpi {
+    const double* __restrict__ y;
+    const double* __restrict__ y_restart;
+    const double* __restrict__ rl;
+    const double* __restrict__ ru;
+    double* __restrict__ ax_out;  // may be null
+    double* __restrict__ partial;
+    using Acc = Slots<4, 0xFu>;
+    __device__ __forceinline__ void row(int i, double axi, Acc& acc) const {
+        if (ax_out) ax_out[i] = axi;
+        const double lo = rl[i], hi = ru[i], yi = y[i];
+        const double pr = axi - clampf(axi, lo, hi);
+        acc.add(0, pr * pr);
+        acc.add(1, yi * yi);
+        const double dy = yi - y_restart[i];
+        acc.add(2, dy * dy);
+        double support = 0.0;
+        if (yi > 0.0) support = isfinite(hi) ? yi * hi : 0.0;
+        else if (yi < 0.0) support = isfinite(lo) ? yi * lo : 0.0;
+        acc.add(3, -support);
+    }
+    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
+};
+
+// Column slots (sums): 0 dual violation^2, 1 dual objective column terms,
+// 2 c'x, 3 |x|^2, 4 |x - x_restart|^2.
+struct ResColsEpi {
+    const double* __restrict__ x;
+    const double* __restrict__ x_restart;
+    const double* __restrict__ c;
+    const double* __restrict__ cl;
+    const double* __restrict__ cu;
+    double* __restrict__ partial;
+    using Acc = Slots<5, 0x1Fu>;
+    __device__ __forceinline__ void row(int j, double aty, Acc& acc) const {
+        const double xj = x[j], lo = cl[j], hi = cu[j];
+        const double r = c[j] + aty;
+        acc.add(2, c[j] * xj);
+        acc.add(3, xj * xj);
+        const double dx = xj - x_restart[j];
+        acc.add(4, dx * dx);
+        const bool lf = isfinite(lo), hf = isfinite(hi);
+        double viol = 0.0, term = 0.0;
+        if (lf && hf) {
+            term = fmin(r * lo, r * hi);
+        } else if (lf) {
+            viol = fmax(0.0, -r);
+            term = fmax(0.0, r) * lo;
+        } else if (hf) {
+            viol = fmax(0.0, r);
+            term = fmin(0.0, r) * hi;
+        } else {
+            viol = fabs(r);
+        }
+        acc.add(0, viol * viol);
+        acc.add(1, term);
+    }
+    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
+};
+
+// out[0..7] in the reference's PdlpResiduals order (PdlpKernels.cuh), plus a
+// copy of the step state; clears the accept flag after the window commit.
+__global__ void k_res_combine(const double* __restrict__ prow, int nrow_blocks, const double* __restrict__ pcol,
+                              int ncol_blocks, double* __restrict__ out, PdlpState* st, int clear_accept) {
+    __shared__ double red[9][kThreads];
+    double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int g = threadIdx.x; g < nrow_blocks; g += kThreads)
+        for (int k = 0; k < 4; ++k) v[k] += prow[g * 4 + k];
+    for (int g = threadIdx.x; g < ncol_blocks; g += kThreads)
+        for (int k = 0; k < 5; ++k) v[4 + k] += pcol[g * 5 + k];
+    for (int k = 0; k < 9; ++k) red[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int k = 0; k < 9; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        // primal_residual_sq, dual_residual_sq, primal_objective, dual_objective,
+        // x_norm_sq, y_norm_sq, primal_move_sq, dual_move_sq
+        out[0] = red[0][0];
+        out[1] = red[4][0];
+        out[2] = red[6][0];
+        out[3] = red[5][0] + red[3][0];
+        out[4] = red[7][0];
+        out[5] = red[1][0];
+        out[6] = red[8][0];
+        out[7] = red[2][0];
+        out[8] = st->eta;
+        out[9] = st->accept_count;
+        out[10] = st->updates;
+        out[11] = st->omega;
+        if (clear_accept) st->accepted = 0.0;
+    }
+}
+
+// x_avg = (1/terms) x_sum (GpuPdlp.cpp:371-390 with the divisor on the device)
+__global__ void k_average(int n, int m, const PdlpState* __restrict__ st, int adaptive, const double* __restrict__ x_sum,
+                          const double* __restrict__ y_sum, double* __restrict__ x_avg, double* __restrict__ y_avg) {
+    double terms = adaptive ? st->accept_count - st->accepted_at_restart : st->terms_fixed;
+    if (terms < 1.0) terms = 1.0;
+    const double scale = 1.0 / terms;
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) x_avg[j] = scale * x_sum[j];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y_avg[i] = scale * y_sum[i];
+}
+
+// Restart (GpuPdlp.cpp:453-497) as one elementwise pass.
+__global__ void k_restart(int n, int m, int to_average, int adaptive, double* __restrict__ x, double* __restrict__ y,
+                          double* __restrict__ x_bar, const double* __restrict__ x_avg,
+                          const double* __restrict__ y_avg, double* __restrict__ ax, double* __restrict__ ax_prev,
+                          const double* __restrict__ ax_avg, double* __restrict__ x_sum, double* __restrict__ y_sum,
+                          double* __restrict__ x_restart, double* __restrict__ y_restart, PdlpState* st) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        double xj = x[j];
+        if (to_average) { xj = x_avg[j]; x[j] = xj; }
+        x_bar[j] = xj;
+        x_sum[j] = 0.0;
+        x_restart[j] = xj;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        double yi = y[i];
+        if (to_average) { yi = y_avg[i]; y[i] = yi; }
+        y_sum[i] = 0.0;
+        y_restart[i] = yi;
+        if (adaptive) {
+            double a = ax[i];
+            if (to_average) { a = ax_avg[i]; ax[i] = a; }
+            ax_prev[i] = a;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && adaptive) st->accepted_at_restart = st->accept_count;
+}
+
+__global__ void k_init_state(PdlpState* st, double eta, double omega, double eta_min, double eta_max) {
+    st->eta = eta;
+    st->omega = omega;
+    st->accepted = 0.0;
+    st->updates = 0.0;
+    st->accept_count = 0.0;
+    st->accepted_at_restart = 0.0;
+    st->eta_min = eta_min;
+    st->eta_max = eta_max;
+    st->terms_fixed = 1.0;
+    st->eta_bar = eta;
+    st->dx_sq = st->dy_sq = st->interaction = 0.0;
+    st->ticket = 0u;
+    st->pad = 0u;
+}
+
+__global__ void k_set_omega(PdlpState* st, double omega, double terms_fixed) {
+    st->omega = omega;
+    st->terms_fixed = terms_fixed;
+}
+
+// ----------------------------------------------------------- norms / power it.
+
+// Sum of squares of v over finite entries below 1e30 in magnitude (block partials).
+__global__ void k_sumsq(const double* __restrict__ v, int n, int finite_only, double* __restrict__ partial) {
+    __shared__ double smem[kWarps];
+    Slots<1, 1u> acc;
+    acc.init();
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x) {
+        const double a = v[j];
+        if (!finite_only || (isfinite(a) && fabs(a) < 1e30)) acc.add(0, a * a);
+    }
+    block_store(acc, partial, smem);
+}
+
+__global__ void k_normalize(double* __restrict__ v, int n, const double* __restrict__ norm_sq) {
+    const double nrm = sqrt(*norm_sq);
+    if (!(nrm > 0.0)) return;
+    const double inv = 1.0 / nrm;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x) v[j] *= inv;
+}
+
+// ----------------------------------------------------------------- scaling
+
+// One warp per CSR row: out[r] = rs[r] * max_p |val[p]| * cs[idx[p]]  (mode 0, Ruiz norms)
+//                       out[r] = sum_p |val[p]| * rs[r] * cs[idx[p]]  (mode 1, Pock-Chambolle alpha=1)
+//                       out[r] = min, out2[r] = max of |val| rs cs     (mode 2, geometric passes)
+__global__ void k_row_stats(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
+                            const double* __restrict__ val, const double* __restrict__ rs,
+                            const double* __restrict__ cs, int mode, double* __restrict__ out,
+                            double* __restrict__ out2) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int r = warp; r < rows; r += nwarps) {
+        const double rsr = rs[r];
+        double a = mode == 2 ? INFINITY : 0.0, b = 0.0;
+        for (int p = ptr[r] + lane; p < ptr[r + 1]; p += 32) {
+            if (mode == 0) {
+                a = fmax(a, fabs(val[p]) * cs[idx[p]]);
+            } else if (mode == 1) {
+                const double v = fabs(val[p]);
+                if (v != 0.0) a += v * rsr * cs[idx[p]];
+            } else {
+                const double v = fabs(val[p]) * rsr * cs[idx[p]];
+                if (v > 0.0) { a = fmin(a, v); b = fmax(b, v); }
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const double oa = __shfl_xor_sync(0xffffffffu, a, off);
+            const double ob = __shfl_xor_sync(0xffffffffu, b, off);
+            a = mode == 0 ? fmax(a, oa) : (mode == 1 ? a + oa : fmin(a, oa));
+            b = fmax(b, ob);
+        }
+        if (lane == 0) {
+            if (mode == 0) out[r] = rsr * a;
+            else if (mode == 1) out[r] = a;
+            else { out[r] = b > 0.0 ? a : 0.0; out2[r] = b; }
+        }
+    }
+}
+
+// max |norm - 1| over positive norms (Scaling.cpp:64-72), block partials.
+__global__ void k_ruiz_dev(const double* __restrict__ rn, int m, const double* __restrict__ cn, int n,
+                           double* __restrict__ partial) {
+    __shared__ double smem[kWarps];
+    Slots<1, 0u> acc;
+    acc.init();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m + n; i += blockDim.x * gridDim.x) {
+        const double v = i < m ? rn[i] : cn[i - m];
+        if (v > 0.0) acc.max(0, fabs(v - 1.0));
+    }
+    block_store(acc, partial, smem);
+}
+
+__global__ void k_div_sqrt(double* __restrict__ s, const double* __restrict__ nrm, int n) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x)
+        if (nrm[j] > 0.0) s[j] /= sqrt(nrm[j]);
+}
+
+__global__ void k_mul_into(double* __restrict__ s, const double* __restrict__ t, int n) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x) s[j] *= t[j];
+}
+
+__global__ void k_inv_sqrt_or_one(double* __restrict__ s, const double* __restrict__ acc, int n) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x)
+        s[j] = acc[j] > 0.0 ? 1.0 / sqrt(acc[j]) : 1.0;
+}
+
+__global__ void k_geo_update(double* __restrict__ s, const double* __restrict__ mn, const double* __restrict__ mx, int n) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x)
+        if (mx[j] > 0.0) s[j] /= sqrt(mn[j] * mx[j]);
+}
+
+// sk_scale.c:59-70: round to the power of two just below-or-at half the mantissa.
+__global__ void k_round_pow2(double* __restrict__ s, int n) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x) {
+        const double v = s[j];
+        if (!(v > 0.0) || !isfinite(v)) { s[j] = 1.0; continue; }
+        int e;
+        frexp(v, &e);
+        s[j] = ldexp(1.0, e - 1);
+    }
+}
+
+__global__ void k_fill_d(double* __restrict__ v, double value, int n) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x) v[j] = value;
+}
+
+// Scaled values of a CSR: out[p] = (val[p] * rs[r]) * cs[idx[p]] (Scaling.cpp:94-109)
+// transposed = 1 swaps the roles so A^T gets bit-identical values.
+__global__ void k_scale_values(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
+                               const double* __restrict__ val, const double* __restrict__ rs,
+                               const double* __restrict__ cs, int transposed, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int r = warp; r < rows; r += nwarps)
+        for (int p = ptr[r] + lane; p < ptr[r + 1]; p += 32)
+            out[p] = transposed ? (val[p] * rs[idx[p]]) * cs[r] : (val[p] * rs[r]) * cs[idx[p]];
+}
+
+// Scaled model vectors (LpSolver.cpp:74-91); |bound| >= 1e30 becomes +-inf.
+__global__ void k_scale_vectors(int n, int m, const double* __restrict__ R, const double* __restrict__ Cs,
+                                double* __restrict__ c, double* __restrict__ cl, double* __restrict__ cu,
+                                double* __restrict__ rl, double* __restrict__ ru) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const double s = Cs[j];
+        c[j] = c[j] * s;
+        const double lo = cl[j], hi = cu[j];
+        cl[j] = lo <= -1e30 ? -INFINITY : lo / s;
+        cu[j] = hi >= 1e30 ? INFINITY : hi / s;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const double s = R[i];
+        const double lo = rl[i], hi = ru[i];
+        rl[i] = lo <= -1e30 ? -INFINITY : s * lo;
+        ru[i] = hi >= 1e30 ? INFINITY : s * hi;
+    }
+}
+
+__global__ void k_unscale(int n, int m, const double* __restrict__ Cs, const double* __restrict__ R,
+                          double* __restrict__ x, double* __restrict__ y) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) x[j] = x[j] * Cs[j];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y[i] = y[i] * R[i];
+}
+
+// warm start: x' = x / C, y' = y / R
+__global__ void k_to_scaled(int n, int m, const double* __restrict__ Cs, const double* __restrict__ R,
+                            double* __restrict__ x, double* __restrict__ y) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) x[j] = x[j] / Cs[j];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y[i] = y[i] / R[i];
+}
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Kkt {
+    double primal = 1, dual = 1, gap = 1, pobj = 0, dobj = 0, pmove = 0, dmove = 0;
+    double worst() const { return std::max(std::max(primal, dual), gap); }
+};
+
+Kkt to_kkt(const double* r, double cost_norm, double bound_norm) {
+    Kkt k;
+    k.primal = std::sqrt(std::max(0.0, r[0])) / (1.0 + bound_norm);
+    k.dual = std::sqrt(std::max(0.0, r[1])) / (1.0 + cost_norm);
+    k.pobj = r[2];
+    k.dobj = r[3];
+    k.gap = std::fabs(r[2] - r[3]) / (1.0 + std::fabs(r[2]) + std::fabs(r[3]));
+    k.pmove = std::sqrt(std::max(0.0, r[6]));
+    k.dmove = std::sqrt(std::max(0.0, r[7]));
+    if (!std::isfinite(k.primal) || !std::isfinite(k.dual) || !std::isfinite(k.gap))
+        k.primal = k.dual = k.gap = std::numeric_limits<double>::infinity();
+    return k;
+}
+
+struct PdlpRun {
+    int n = 0, m = 0, sms = 148;
+    cudaStream_t stream = nullptr;
+    TileCsr A, AT;  // scaled views
+    DevBuf blob, vals;
+    double *c, *cl, *cu, *rl, *ru, *R, *Cs, *tmp_n, *tmp_m, *tmp2_m;
+    double *x, *x_cand, *x_sum, *x_avg, *x_restart, *x_bar, *aty;
+    double *y, *y_cand, *y_sum, *y_avg, *y_restart, *ax, *ax_prev, *ax_cand, *ax_avg;
+    double *part_a, *part_b, *part_c, *res, *scalar;
+    PdlpState* st;
+    double* host;
+    int grid_k2 = 1, grid_k3 = 1, grid_rr = 1, grid_rc = 1, grid_df = 1, grid_pf = 1;
+    int launches = 0;
+    std::vector<cudaGraphExec_t> graphs;
+    ~PdlpRun() {
+        for (auto g : graphs)
+            if (g) cudaGraphExecDestroy(g);
+    }
+
+    int allocate(const Plan& plan) {
+        n = plan.a.cols;
+        m = plan.a.rows;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan.device);
+        const size_t nb = (static_cast<size_t>(n) * 8 + 255) / 256 * 256;
+        const size_t mb = (static_cast<size_t>(m) * 8 + 255) / 256 * 256;
+        const size_t pb = (static_cast<size_t>(sms) * 8 * 8 * 8 + 255) / 256 * 256;
+        if (blob.alloc(13 * nb + 16 * mb + 3 * pb + 4096, "cudaMalloc PDLP workspace")) return -1;
+        if (vals.alloc(static_cast<size_t>(plan.a.nnz) * 16 + 512, "cudaMalloc scaled values")) return -1;
+        char* p = blob.as<char>();
+        auto take = [&](size_t b) { double* r = reinterpret_cast<double*>(p); p += b; return r; };
+        c = take(nb); cl = take(nb); cu = take(nb); Cs = take(nb); tmp_n = take(nb);
+        x = take(nb); x_cand = take(nb); x_sum = take(nb); x_avg = take(nb); x_restart = take(nb);
+        x_bar = take(nb); aty = take(nb); take(nb);
+        rl = take(mb); ru = take(mb); R = take(mb); tmp_m = take(mb); tmp2_m = take(mb);
+        y = take(mb); y_cand = take(mb); y_sum = take(mb); y_avg = take(mb); y_restart = take(mb);
+        ax = take(mb); ax_prev = take(mb); ax_cand = take(mb); ax_avg = take(mb); take(mb); take(mb);
+        part_a = take(pb); part_b = take(pb); part_c = take(pb);
+        res = take(1024);
+        scalar = take(1024);
+        st = reinterpret_cast<PdlpState*>(take(1024));
+        (void)tmp2_m;
+        A = plan.a;
+        AT = plan.at;
+        A.val = vals.as<double>();
+        AT.val = vals.as<double>() + ((static_cast<size_t>(plan.a.nnz) + 63) / 64 * 64);
+        return 0;
+    }
+
+    int eg(int len) const { return elem_grid(std::max(len, 1)); }
+
+    double sumsq(const double* v, int len, bool finite_only) {
+        const int g = std::min(eg(len), sms * 4);
+        k_sumsq<<<g, kThreads, 0, stream>>>(v, len, finite_only ? 1 : 0, part_a);
+        k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part_a, len > 0 ? g : 0, scalar);
+        launches += 2;
+        double h = 0;
+        cudaMemcpyAsync(host, scalar, sizeof(double), cudaMemcpyDeviceToHost, stream);
+        cudaStreamSynchronize(stream);
+        h = host[0];
+        return h;
+    }
+
+    // Ruiz (Scaling.cpp:11-92), then Pock-Chambolle on the Ruiz-scaled matrix,
+    // composed (Scaling.cpp:147-152); or the power-of-two passes (sk_scale.c).
+    int scale(const Plan& plan, int mode, int ruiz_iters, double ruiz_tol, int* syncs) {
+        const int gm = eg(m), gn = eg(n);
+        const int wg_m = std::min((m + 7) / 8 + 1, sms * 16), wg_n = std::min((n + 7) / 8 + 1, sms * 16);
+        k_fill_d<<<gm, kThreads, 0, stream>>>(R, 1.0, m);
+        k_fill_d<<<gn, kThreads, 0, stream>>>(Cs, 1.0, n);
+        const bool any = (mode & (SANKHYA_B200_SCALE_RUIZ | SANKHYA_B200_SCALE_POCK_CHAMBOLLE | SANKHYA_B200_SCALE_POW2)) != 0;
+        if (any && plan.a.nnz > 0 && m > 0 && n > 0) {
+            if (mode & SANKHYA_B200_SCALE_POW2) {
+                for (int pass = 0; pass < 4; ++pass) {
+                    // columns first (sk_scale.c:38-47), then rows (:48-57)
+                    k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 2,
+                                                               tmp_n, x_avg);
+                    k_geo_update<<<gn, kThreads, 0, stream>>>(Cs, tmp_n, x_avg, n);
+                    k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 2,
+                                                               tmp_m, y_avg);
+                    k_geo_update<<<gm, kThreads, 0, stream>>>(R, tmp_m, y_avg, m);
+                    launches += 4;
+                }
+                k_round_pow2<<<gm, kThreads, 0, stream>>>(R, m);
+                k_round_pow2<<<gn, kThreads, 0, stream>>>(Cs, n);
+            }
+            if (mode & SANKHYA_B200_SCALE_RUIZ) {
+                // factors accumulate in (R, Cs); identity restored if not converged
+                bool converged = false;
+                for (int it = 0; it < ruiz_iters; ++it) {
+                    k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 0,
+                                                               tmp_m, nullptr);
+                    k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 0,
+                                                               tmp_n, nullptr);
+                    const int g = std::min(eg(m + n), sms * 4);
+                    k_ruiz_dev<<<g, kThreads, 0, stream>>>(tmp_m, m, tmp_n, n, part_a);
+                    k_combine<1, 0u><<<1, kThreads, 0, stream>>>(part_a, g, scalar);
+                    launches += 4;
+                    cudaMemcpyAsync(host, scalar, sizeof(double), cudaMemcpyDeviceToHost, stream);
+                    B200_TRY(cudaStreamSynchronize(stream), "Ruiz");
+                    ++*syncs;
+                    if (host[0] < ruiz_tol) { converged = true; break; }
+                    k_div_sqrt<<<gm, kThreads, 0, stream>>>(R, tmp_m, m);
+                    k_div_sqrt<<<gn, kThreads, 0, stream>>>(Cs, tmp_n, n);
+                }
+                if (!converged && !(mode & SANKHYA_B200_SCALE_POW2)) {
+                    k_fill_d<<<gm, kThreads, 0, stream>>>(R, 1.0, m);
+                    k_fill_d<<<gn, kThreads, 0, stream>>>(Cs, 1.0, n);
+                }
+            }
+            if (mode & SANKHYA_B200_SCALE_POCK_CHAMBOLLE) {
+                k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 1, tmp_m,
+                                                           nullptr);
+                k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 1, tmp_n,
+                                                           nullptr);
+                k_inv_sqrt_or_one<<<gm, kThreads, 0, stream>>>(tmp2_m, tmp_m, m);
+                k_inv_sqrt_or_one<<<gn, kThreads, 0, stream>>>(x_avg, tmp_n, n);
+                k_mul_into<<<gm, kThreads, 0, stream>>>(R, tmp2_m, m);
+                k_mul_into<<<gn, kThreads, 0, stream>>>(Cs, x_avg, n);
+                launches += 6;
+            }
+        }
+        k_scale_values<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 0,
+                                                      const_cast<double*>(A.val));
+        k_scale_values<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, R, Cs, 1,
+                                                      const_cast<double*>(AT.val));
+        k_scale_vectors<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, R, Cs, c, cl, cu, rl, ru);
+        launches += 3;
+        B200_TRY(cudaGetLastError(), "scaling launch");
+        return 0;
+    }
+
+    // GpuPdlp.cpp:179-211 on the device, one sync at the end.
+    double power_norm(int iters) {
+        const int g = std::min(eg(n), sms * 4);
+        k_fill_d<<<eg(n), kThreads, 0, stream>>>(x_avg, 1.0, n);
+        k_sumsq<<<g, kThreads, 0, stream>>>(x_avg, n, 0, part_a);
+        k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part_a, n > 0 ? g : 0, scalar);
+        k_normalize<<<eg(n), kThreads, 0, stream>>>(x_avg, n, scalar);
+        const int ga = tiled_grid<StoreEpi>(A), gt = tiled_grid<StoreEpi>(AT);
+        for (int k = 0; k < iters; ++k) {
+            launch_tiled(A, x_avg, StoreEpi{ax_avg}, stream, ga);
+            launch_tiled(AT, ax_avg, StoreEpi{x_bar}, stream, gt);
+            k_sumsq<<<g, kThreads, 0, stream>>>(x_bar, n, 0, part_a);
+            k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part_a, n > 0 ? g : 0, scalar);
+            k_copy<<<eg(n), kThreads, 0, stream>>>(x_avg, x_bar, n);
+            k_normalize<<<eg(n), kThreads, 0, stream>>>(x_avg, n, scalar);
+        }
+        launches += 4 + 6 * iters;
+        cudaMemcpyAsync(host, scalar, sizeof(double), cudaMemcpyDeviceToHost, stream);
+        cudaStreamSynchronize(stream);
+        const double lambda = std::sqrt(std::max(0.0, host[0]));
+        const double norm = std::sqrt(lambda);
+        return (norm > 0.0 && std::isfinite(norm)) ? norm : 1.0;
+    }
+
+    void residuals(const double* xv, const double* yv, double* ax_out, double* out, int clear_accept) {
+        const int nbr = A.ntiles ? grid_rr : 0, nbc = AT.ntiles ? grid_rc : 0;
+        launch_tiled(A, xv, ResRowsEpi{yv, y_restart, rl, ru, ax_out, part_a}, stream, grid_rr);
+        launch_tiled(AT, yv, ResColsEpi{xv, x_restart, c, cl, cu, part_b}, stream, grid_rc);
+        k_res_combine<<<1, kThreads, 0, stream>>>(part_a, nbr, part_b, nbc, out, st, clear_accept);
+        launches += 3;
+    }
+
+    void adaptive_iteration(bool make_candidate) {
+        k_commit_dual<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, x, x_cand, x_sum, y, y_cand, y_sum, ax,
+                                                                   ax_prev, ax_cand, rl, ru, make_candidate ? 1 : 0);
+        ++launches;
+        if (!make_candidate) return;
+        launch_tiled(AT, y_cand, PrimalCandEpi{st, x, c, cl, cu, x_cand, part_c}, stream, grid_k2);
+        launch_tiled(A, x_cand,
+                     ProbeEpi{st, y, y_cand, ax, ax_cand, part_a + 4096, part_c, AT.ntiles ? grid_k2 : 0}, stream,
+                     grid_k3);
+        launches += 2;
+    }
+
+    void fixed_iteration(double tau, double sigma) {
+        launch_tiled(A, x_bar, DualFixedEpi{st, y, y_sum, rl, ru, sigma}, stream, grid_df);
+        launch_tiled(AT, y, PrimalFixedEpi{x, x_bar, x_sum, c, cl, cu, tau}, stream, grid_pf);
+        launches += 2;
+    }
+
+    // One window (period iterations) + window-end evaluation, as a graph.
+    int window(int period, bool adaptive, double tau, double sigma, int* graph_slot) {
+        cudaGraphExec_t exec = nullptr;
+        if (*graph_slot >= 0) exec = graphs[static_cast<size_t>(*graph_slot)];
+        if (!exec) {
+            const int saved = launches;
+            cudaGraph_t g;
+            B200_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            for (int k = 0; k < period; ++k) {
+                if (adaptive) adaptive_iteration(true);
+                else fixed_iteration(tau, sigma);
+            }
+            if (adaptive) adaptive_iteration(false);  // commit the last probe
+            residuals(x, y, nullptr, res, 0);
+            k_average<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, adaptive ? 1 : 0, x_sum, y_sum, x_avg,
+                                                                    y_avg);
+            residuals(x_avg, y_avg, ax_avg, res + 16, 1);
+            cudaMemcpyAsync(host, res, 32 * sizeof(double), cudaMemcpyDeviceToHost, stream);
+            B200_TRY(cudaStreamEndCapture(stream, &g), "end capture");
+            cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail_cuda("graph instantiate", e);
+            graphs.push_back(exec);
+            *graph_slot = static_cast<int>(graphs.size()) - 1;
+            launches = saved;
+        }
+        B200_TRY(cudaGraphLaunch(exec, stream), "graph launch");
+        launches += (adaptive ? 3 * period + 1 : 2 * period) + 7;
+        return 0;
+    }
+};
+
+}  // namespace
+
+}  // namespace b200
+
+using namespace b200;
+
+extern "C" void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* s) {
+    if (!s) return;
+    std::memset(s, 0, sizeof(*s));
+    s->struct_version = 1;
+    s->max_iterations = 500000;
+    s->restart_period = 64;
+    s->power_iterations = 30;
+    s->adaptive_step = 1;
+    s->scaling = SANKHYA_B200_SCALE_RUIZ | SANKHYA_B200_SCALE_POCK_CHAMBOLLE;
+    s->ruiz_iterations = 100;
+    s->precision = SANKHYA_B200_FP64;
+    s->eps_optimal = 1e-8;
+    s->time_limit = 0.0;
+    s->eta_min_factor = 1e-6;
+    s->eta_max_factor = 1e4;
+    s->ruiz_tolerance = 1e-2;
+}
+
+extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const double* c, const double* row_lower,
+                                       const double* row_upper, const double* col_lower, const double* col_upper,
+                                       const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
+                                       double* x_out, double* y_out, SankhyaB200PdlpResult* result) {
+    clear_error();
+    (void)cudaGetLastError();  // a caller's earlier non-sticky error is not ours
+    if (!result) return fail_msg("null result");
+    std::memset(result, 0, sizeof(*result));
+    result->status = -1;
+    SankhyaB200PdlpSettings s;
+    sankhya_b200_pdlp_default_settings(&s);
+    if (settings) {
+        if (settings->struct_version != 1) return fail_msg("unsupported settings struct_version");
+        s = *settings;
+    }
+    if (!matrix || !c || !row_lower || !row_upper || !col_lower || !col_upper || !x_out)
+        return fail_msg("null model or output pointer");
+    if (s.max_iterations <= 0 || s.restart_period <= 0 || s.power_iterations < 0 || !(s.eps_optimal > 0.0) ||
+        s.time_limit < 0.0 || !(s.eta_min_factor > 0.0) || !(s.eta_max_factor >= s.eta_min_factor) ||
+        s.ruiz_iterations < 0 || (s.precision != SANKHYA_B200_FP64 && s.precision != SANKHYA_B200_FP32_REFINE))
+        return fail_msg("invalid PDLP settings");
+    const int n = matrix->cols, m = matrix->rows;
+    for (int j = 0; j < n; ++j)
+        if (!std::isfinite(c[j]) || std::isnan(col_lower[j]) || std::isnan(col_upper[j]) || col_lower[j] > col_upper[j])
+            return fail_msg("invalid cost or column bound");
+    for (int i = 0; i < m; ++i)
+        if (std::isnan(row_lower[i]) || std::isnan(row_upper[i]) || row_lower[i] > row_upper[i])
+            return fail_msg("invalid row bound");
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) return fail_msg("no CUDA device available");
+    const double t_start = now_s();
+    std::shared_ptr<Plan> plan;
+    if (get_plan(matrix, &plan)) return -1;
+    PdlpRun run;
+    run.stream = engine_stream();
+    if (run.allocate(*plan)) return -1;
+    struct HostSlot {
+        double* p = nullptr;
+        ~HostSlot() { if (p) cudaFreeHost(p); }
+    } hs;
+    B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&hs.p), 64 * sizeof(double)), "cudaMallocHost");
+    run.host = hs.p;
+    cudaStream_t stream = run.stream;
+    const size_t nb = sizeof(double) * static_cast<size_t>(n), mb = sizeof(double) * static_cast<size_t>(m);
+    if (n) {
+        B200_TRY(cudaMemcpyAsync(run.c, c, nb, cudaMemcpyHostToDevice, stream), "upload c");
+        B200_TRY(cudaMemcpyAsync(run.cl, col_lower, nb, cudaMemcpyHostToDevice, stream), "upload col_lower");
+        B200_TRY(cudaMemcpyAsync(run.cu, col_upper, nb, cudaMemcpyHostToDevice, stream), "upload col_upper");
+    }
+    if (m) {
+        B200_TRY(cudaMemcpyAsync(run.rl, row_lower, mb, cudaMemcpyHostToDevice, stream), "upload row_lower");
+        B200_TRY(cudaMemcpyAsync(run.ru, row_upper, mb, cudaMemcpyHostToDevice, stream), "upload row_upper");
+    }
+    int syncs = 0;
+    if (run.scale(*plan, s.scaling, s.ruiz_iterations, s.ruiz_tolerance, &syncs)) return -1;
+
+    // norms of the scaled data (GpuPdlp.cpp:94-99), finite entries only
+    const double cost_norm = std::sqrt(run.sumsq(run.c, n, true));
+    const double bl = run.sumsq(run.rl, m, true), bu = run.sumsq(run.ru, m, true);
+    const double bound_norm = std::sqrt(bl + bu);
+    syncs += 3;
+    const double matrix_norm = run.power_norm(s.power_iterations);
+    ++syncs;
+    const double eta_global = kStepSafety / matrix_norm;
+    const double eta_min = s.eta_min_factor / matrix_norm, eta_max = s.eta_max_factor / matrix_norm;
+    double omega = 1.0;
+    if (cost_norm > 0.0 && bound_norm > 0.0) omega = std::min(kMaxWeight, std::max(kMinWeight, cost_norm / bound_norm));
+
+    // initial iterate: zeros or the warm start (moved into the scaled space)
+    B200_TRY(cudaMemsetAsync(run.x, 0, std::max<size_t>(nb, 1), stream), "zero");
+    B200_TRY(cudaMemsetAsync(run.y, 0, std::max<size_t>(mb, 1), stream), "zero");
+    if (x0 && n) B200_TRY(cudaMemcpyAsync(run.x, x0, nb, cudaMemcpyHostToDevice, stream), "upload x0");
+    if (y0 && m) B200_TRY(cudaMemcpyAsync(run.y, y0, mb, cudaMemcpyHostToDevice, stream), "upload y0");
+    if (x0 || y0) k_to_scaled<<<run.eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, run.Cs, run.R, run.x, run.y);
+    for (double* v : {run.x_sum, run.x_cand, run.x_avg, run.aty}) cudaMemsetAsync(v, 0, std::max<size_t>(nb, 1), stream);
+    for (double* v : {run.y_sum, run.y_cand, run.y_avg, run.ax_cand, run.ax_avg})
+        cudaMemsetAsync(v, 0, std::max<size_t>(mb, 1), stream);
+    B200_TRY(cudaMemcpyAsync(run.x_restart, run.x, std::max<size_t>(nb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
+    B200_TRY(cudaMemcpyAsync(run.x_bar, run.x, std::max<size_t>(nb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
+    B200_TRY(cudaMemcpyAsync(run.y_restart, run.y, std::max<size_t>(mb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
+    // A x of the start point; the first extrapolation is then the identity
+    if (m) launch_tiled(run.A, run.x, StoreEpi{run.ax}, stream, tiled_grid<StoreEpi>(run.A));
+    B200_TRY(cudaMemcpyAsync(run.ax_prev, run.ax, std::max<size_t>(mb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
+    k_init_state<<<1, 1, 0, stream>>>(run.st, eta_global, omega, eta_min, eta_max);
+    B200_TRY(cudaGetLastError(), "PDLP setup");
+
+    run.grid_k2 = tiled_grid<PrimalCandEpi>(run.AT);
+    run.grid_k3 = tiled_grid<ProbeEpi>(run.A);
+    run.grid_rr = tiled_grid<ResRowsEpi>(run.A);
+    run.grid_rc = tiled_grid<ResColsEpi>(run.AT);
+    run.grid_df = tiled_grid<DualFixedEpi>(run.A);
+    run.grid_pf = tiled_grid<PrimalFixedEpi>(run.AT);
+    const bool adaptive = s.adaptive_step != 0;
+    // The probe's last-block combine needs every tile of A to launch a block.
+    if (adaptive && run.A.ntiles == 0 && m == 0) {
+        // no rows: the interaction is zero and every step is accepted; handled by the generic path
+    }
+
+    TimingState& ts = timing();
+    ts.last = SankhyaB200Timing{};
+    int iteration = 0, windows_since_restart = 0, iterations_since_restart = 0, restarts = 0;
+    double mu_at_restart = std::numeric_limits<double>::infinity(), mu_previous = mu_at_restart;
+    Kkt best;
+    bool converged = false, timed_out = false, numeric = false;
+    int slot_full = -1, slot_tail = -1;
+    double eta_host = eta_global, accept_count = 0, updates = 0;
+    while (iteration < s.max_iterations) {
+        const int period = std::min(s.restart_period, s.max_iterations - iteration);
+        if (period <= 0) break;
+        const double terms_fixed = static_cast<double>((windows_since_restart + 1) * s.restart_period);
+        k_set_omega<<<1, 1, 0, stream>>>(run.st, omega, terms_fixed);
+        const double tau = eta_global / omega, sigma = eta_global * omega;
+        // the fixed path bakes tau/sigma into the graph: rebuild it when omega moves
+        int* slot = period == s.restart_period ? &slot_full : &slot_tail;
+        if (!adaptive && *slot >= 0) {
+            cudaGraphExecDestroy(run.graphs[static_cast<size_t>(*slot)]);
+            run.graphs[static_cast<size_t>(*slot)] = nullptr;
+        }
+        if (run.window(period, adaptive, tau, sigma, slot)) return -1;
+        B200_TRY(cudaStreamSynchronize(stream), "PDLP window");
+        ++syncs;
+        iteration += period;
+        iterations_since_restart += period;
+        ++windows_since_restart;
+        const double* h = run.host;
+        const Kkt current = to_kkt(h, cost_norm, bound_norm);
+        const Kkt average = to_kkt(h + 16, cost_norm, bound_norm);
+        eta_host = h[16 + 8];
+        accept_count = h[16 + 9];
+        updates = h[16 + 10];
+        const bool average_better = average.worst() < current.worst();
+        best = average_better ? average : current;
+        if (!std::isfinite(current.primal) && !std::isfinite(average.primal)) {
+            numeric = true;
+            break;
+        }
+        if (best.primal <= s.eps_optimal && best.dual <= s.eps_optimal && best.gap <= s.eps_optimal) {
+            if (average_better) {
+                B200_TRY(cudaMemcpyAsync(run.x, run.x_avg, std::max<size_t>(nb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
+                B200_TRY(cudaMemcpyAsync(run.y, run.y_avg, std::max<size_t>(mb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
+            }
+            converged = true;
+            break;
+        }
+        if (s.time_limit > 0.0 && now_s() - t_start > s.time_limit) {
+            timed_out = true;
+            break;
+        }
+        const double mu = best.worst();
+        const bool sufficient = mu <= kSufficient * mu_at_restart;
+        const bool necessary = mu <= kNecessary * mu_at_restart && mu > mu_previous;
+        const bool artificial = static_cast<double>(iterations_since_restart) >= kArtificial * static_cast<double>(iteration);
+        mu_previous = mu;
+        if (!(sufficient || necessary || artificial)) continue;
+        k_restart<<<run.eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, average_better ? 1 : 0, adaptive ? 1 : 0,
+                                                                   run.x, run.y, run.x_bar, run.x_avg, run.y_avg,
+                                                                   run.ax, run.ax_prev, run.ax_avg, run.x_sum,
+                                                                   run.y_sum, run.x_restart, run.y_restart, run.st);
+        ++run.launches;
+        windows_since_restart = 0;
+        iterations_since_restart = 0;
+        mu_at_restart = mu;
+        mu_previous = std::numeric_limits<double>::infinity();
+        ++restarts;
+        if (best.pmove > 1e-14 && best.dmove > 1e-14) {
+            const double target = best.dmove / best.pmove;
+            const double updated = std::exp(kSmoothing * std::log(target) + (1.0 - kSmoothing) * std::log(omega));
+            if (std::isfinite(updated)) omega = std::min(kMaxWeight, std::max(kMinWeight, updated));
+        }
+    }
+    // back to the caller's space
+    k_unscale<<<run.eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, run.Cs, run.R, run.x, run.y);
+    if (n) B200_TRY(cudaMemcpyAsync(x_out, run.x, nb, cudaMemcpyDeviceToHost, stream), "download x");
+    if (y_out && m) B200_TRY(cudaMemcpyAsync(y_out, run.y, mb, cudaMemcpyDeviceToHost, stream), "download y");
+    B200_TRY(cudaStreamSynchronize(stream), "download");
+    ++syncs;
+    result->status = numeric ? -2 : converged ? 0 : timed_out ? 2 : 1;
+    result->iterations = iteration;
+    result->restarts = restarts;
+    result->rejected_steps = adaptive ? static_cast<int>(std::max(0.0, updates - accept_count)) : 0;
+    result->host_syncs = syncs;
+    result->refinements = 0;
+    result->primal_objective = best.pobj;
+    result->dual_objective = best.dobj;
+    result->relative_primal_residual = best.primal;
+    result->relative_dual_residual = best.dual;
+    result->relative_gap = best.gap;
+    result->matrix_norm = matrix_norm;
+    result->final_step_size = adaptive ? eta_host : eta_global;
+    result->primal_weight = omega;
+    result->seconds = now_s() - t_start;
+    ts.last.iterations = iteration;
+    ts.last.checkpoints = syncs;
+    ts.last.kernel_launches = run.launches;
+    return numeric ? -2 : 0;
+}
