@@ -176,6 +176,17 @@ SANKHYA_CUDA_API int sankhya_b200_pdlp_solve(
     const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
     double* x_out, double* y_out, SankhyaB200PdlpResult* result);
 
+/* Equilibration factors computed on the device, without solving: row_scale
+   (rows) and col_scale (cols) such that the scaled matrix is
+   diag(row_scale) A diag(col_scale). scaling is a SANKHYA_B200_SCALE_* mask:
+   POW2 runs 4 geometric passes rounded to powers of two (c/src/sk_scale.c:20-72),
+   RUIZ the infinity-norm equilibration (src/lp/Scaling.cpp:11-92, identity when it
+   does not reach ruiz_tolerance in ruiz_iterations), POCK_CHAMBOLLE (alpha = 1,
+   Scaling.cpp:111-145) on the result, composed as in src/lp/LpSolver.cpp:62-71. */
+SANKHYA_CUDA_API int sankhya_b200_scale_factors(
+    const SankhyaCudaCSR* matrix, int scaling, int ruiz_iterations, double ruiz_tolerance,
+    double* row_scale, double* col_scale);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,7 +32,7 @@ REFERENCE_SYMBOLS = (
 )
 EXTENSION_SYMBOLS = (
     "sankhya_b200_set_timing", "sankhya_b200_last_timing", "sankhya_b200_pdhg_loop",
-    "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve",
+    "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve", "sankhya_b200_scale_factors",
 )
 
 _lib = None
@@ -160,6 +160,7 @@ def _declare(L):
         L.sankhya_b200_pdlp_default_settings.restype = None
         L.sankhya_b200_pdlp_solve.argtypes = [P(CSR), dptr, dptr, dptr, dptr, dptr, P(PdlpSettings), dptr,
                                               dptr, dptr, dptr, P(PdlpResult)]
+        L.sankhya_b200_scale_factors.argtypes = [P(CSR), C.c_int, C.c_int, C.c_double, dptr, dptr]
 
 
 def _d(a):
@@ -297,3 +298,12 @@ def pdlp_solve(matrix: Matrix, inst, s: PdlpSettings | None = None, x0=None, y0=
     rc = L.sankhya_b200_pdlp_solve(C.byref(matrix.handle), _p(c), _p(rl), _p(ru), _p(cl), _p(cu), C.byref(s),
                                    _p(_d(x0)), _p(_d(y0)), _p(x), _p(y), C.byref(res))
     return rc, x, y, res.as_dict()
+
+
+def scale_factors(matrix: Matrix, scaling: int, ruiz_iterations: int = 100, ruiz_tolerance: float = 1e-2):
+    """Device equilibration factors (row_scale, col_scale) for a device matrix."""
+    r = np.zeros(matrix.handle.rows)
+    c = np.zeros(matrix.handle.cols)
+    rc = lib().sankhya_b200_scale_factors(C.byref(matrix.handle), int(scaling), int(ruiz_iterations),
+                                          float(ruiz_tolerance), _p(r), _p(c))
+    return rc, r, c

@@ -33,26 +33,28 @@ void clear_error() { g_last_error[0] = '\0'; }
 // ------------------------------------------------------------------ tiles
 
 std::vector<int> build_tiles(int rows, const int* ptr) {
-    std::vector<int> tiles;
-    tiles.reserve(static_cast<size_t>(rows) / 64 + 2);
+    std::vector<int> tiles;  // (row, nonzero) pairs
+    tiles.reserve(static_cast<size_t>(rows) / 8 + 4);
     int r = 0;
     while (r < rows) {
         tiles.push_back(r);
+        tiles.push_back(ptr[r]);
         const int len = ptr[r + 1] - ptr[r];
-        if (len > kTileNnz) {
+        if (len > kChunkNnz) {
             ++r;
             continue;
         }
         const int start = r;
         int nnz = 0;
-        while (r < rows && r - start < kMaxTileRows) {
+        while (r < rows && r - start < kChunkRows) {
             const int l = ptr[r + 1] - ptr[r];
-            if (nnz + l > kTileNnz) break;
+            if (nnz + l > kChunkNnz) break;
             nnz += l;
             ++r;
         }
     }
     tiles.push_back(rows);
+    tiles.push_back(ptr[rows]);
     return tiles;
 }
 
@@ -67,7 +69,10 @@ Plan::~Plan() {
     cudaFree(d_at_idx);
     cudaFree(d_at_val);
     cudaFree(d_tile_at);
-    for (void* p : workspace) cudaFree(p);
+    cudaFree(d_err);
+    cudaFree(d_a_idx);
+    cudaFree(d_a_val);
+    solve_cache.reset();
     if (current >= 0 && current != device) cudaSetDevice(current);
 }
 
@@ -111,23 +116,36 @@ int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const
         upload(reinterpret_cast<void**>(&plan->d_at_val), at_val.data(), at_val.size() * sizeof(double), "cudaMalloc A^T values") ||
         upload(reinterpret_cast<void**>(&plan->d_tile_at), tiles_at.data(), tiles_at.size() * sizeof(int), "cudaMalloc tiles(A^T)"))
         return -1;
+    B200_TRY(cudaMalloc(reinterpret_cast<void**>(&plan->d_err), sizeof(unsigned int)), "cudaMalloc error word");
+    B200_TRY(cudaMemset(plan->d_err, 0, sizeof(unsigned int)), "clear error word");
+    const int* a_idx = static_cast<const int*>(m->device_column_indices);
+    const double* a_val = static_cast<const double*>(m->device_values);
+    if ((reinterpret_cast<uintptr_t>(a_idx) | reinterpret_cast<uintptr_t>(a_val)) & 15u) {
+        if (upload(reinterpret_cast<void**>(&plan->d_a_idx), h_idx, static_cast<size_t>(nnz) * sizeof(int), "cudaMalloc A indices") ||
+            upload(reinterpret_cast<void**>(&plan->d_a_val), h_val, static_cast<size_t>(nnz) * sizeof(double), "cudaMalloc A values"))
+            return -1;
+        a_idx = plan->d_a_idx;
+        a_val = plan->d_a_val;
+    }
 
     plan->a.rows = rows;
     plan->a.cols = cols;
     plan->a.nnz = nnz;
     plan->a.ptr = static_cast<const int*>(m->device_row_offsets);
-    plan->a.idx = static_cast<const int*>(m->device_column_indices);
-    plan->a.val = static_cast<const double*>(m->device_values);
-    plan->a.ntiles = static_cast<int>(tiles_a.size()) - 1;
-    plan->a.tile_row = plan->d_tile_a;
+    plan->a.idx = a_idx;
+    plan->a.val = a_val;
+    plan->a.ntiles = static_cast<int>(tiles_a.size()) / 2 - 1;
+    plan->a.tile = reinterpret_cast<const int2*>(plan->d_tile_a);
+    plan->a.err = plan->d_err;
     plan->at.rows = cols;
     plan->at.cols = rows;
     plan->at.nnz = nnz;
     plan->at.ptr = plan->d_at_ptr;
     plan->at.idx = plan->d_at_idx;
     plan->at.val = plan->d_at_val;
-    plan->at.ntiles = static_cast<int>(tiles_at.size()) - 1;
-    plan->at.tile_row = plan->d_tile_at;
+    plan->at.ntiles = static_cast<int>(tiles_at.size()) / 2 - 1;
+    plan->at.tile = reinterpret_cast<const int2*>(plan->d_tile_at);
+    plan->at.err = plan->d_err;
     *out = std::move(plan);
     return 0;
 }
@@ -162,8 +180,8 @@ int get_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out) {
         std::lock_guard<std::mutex> lock(g_registry_mutex);
         auto it = registry().find(m->device_row_offsets);
         if (it != registry().end() && it->second->a.rows == m->rows && it->second->a.cols == m->cols &&
-            it->second->a.nnz == m->nnz && it->second->a.val == m->device_values &&
-            it->second->a.idx == m->device_column_indices) {
+            it->second->a.nnz == m->nnz && (it->second->a.val == m->device_values || it->second->d_a_val) &&
+            (it->second->a.idx == m->device_column_indices || it->second->d_a_idx)) {
             *out = it->second;
             return 0;
         }
@@ -206,7 +224,7 @@ cudaStream_t engine_stream() {
     return state.streams[device];
 }
 
-int grid_for(const void* kernel, int ntiles) {
+int grid_for(const void* kernel, int ntiles, int dynamic_smem) {
     struct Entry { const void* k; int device; int blocks; };
     static std::mutex mu;
     static std::vector<Entry> cache;
@@ -219,7 +237,9 @@ int grid_for(const void* kernel, int ntiles) {
             if (e.k == kernel && e.device == device) resident = e.blocks;
         if (resident == 0) {
             int per_sm = 0, sms = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0);
+            if (dynamic_smem > 48 * 1024)
+                cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dynamic_smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, dynamic_smem);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
             resident = std::max(1, per_sm) * std::max(1, sms);
             cache.push_back({kernel, device, resident});

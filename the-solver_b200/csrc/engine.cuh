@@ -36,14 +36,16 @@ void clear_error();
 
 // ----------------------------------------------------------- tile schedule
 
-constexpr int kThreads = 256;          // threads per tile block
+constexpr int kThreads = 256;          // threads per block (8 warps)
 constexpr int kWarps = kThreads / 32;
-constexpr int kTileNnz = 2048;         // nonzeros staged in shared memory per tile
-constexpr int kShortRow = 32;          // rows up to this length: one thread, sequential sum
-constexpr int kMaxTileRows = 4096;     // cap on rows per tile (keeps empty-row runs balanced)
+constexpr int kChunkNnz = 256;         // nonzeros per warp chunk (8 per lane)
+constexpr int kChunkRows = 32;         // rows per warp chunk (one owning lane each)
+constexpr int kPerLane = kChunkNnz / 32;
+constexpr int kShortRow = 32;          // rows up to this length: owning lane, sequential sum
 
-// Greedy row tiles: consecutive rows whose nonzeros fit kTileNnz; a row longer
-// than kTileNnz is a tile of its own and is reduced by the whole block.
+// Warp chunks: consecutive rows with at most kChunkNnz nonzeros and at most
+// kChunkRows rows; a row longer than kChunkNnz is a chunk of its own. Returns
+// the chunk boundaries as (row, first nonzero) pairs, ntiles + 1 of them.
 std::vector<int> build_tiles(int rows, const int* row_offsets);
 
 struct TileCsr {
@@ -51,7 +53,8 @@ struct TileCsr {
     const int* ptr = nullptr;
     const int* idx = nullptr;
     const double* val = nullptr;
-    const int* tile_row = nullptr;
+    const int2* tile = nullptr;   // chunk boundaries: (first row, first nonzero)
+    unsigned int* err = nullptr;  // counts bounded device waits that gave up (may be null)
 };
 
 // Owns everything a solve needs for one matrix beyond the caller's CSR.
@@ -64,10 +67,12 @@ struct Plan {
     int* d_at_idx = nullptr;
     double* d_at_val = nullptr;
     int* d_tile_at = nullptr;
+    unsigned int* d_err = nullptr;  // wait-timeout counter shared by this plan's launches
+    int* d_a_idx = nullptr;         // owned copies of A when the caller's arrays are
+    double* d_a_val = nullptr;      // not 16-byte aligned (TMA bulk copies need it)
     double row_mass_max = 0.0;   // filled lazily by users that need it
-    std::mutex workspace_mutex;  // serialises solves that share this plan's workspace
-    std::vector<void*> workspace; // cached per-plan device buffers (freed with the plan)
-    size_t workspace_bytes = 0;
+    std::mutex workspace_mutex;   // held by the solve that uses `solve_cache`
+    std::shared_ptr<void> solve_cache; // workspace + captured graphs of the last fixed-step solve
     ~Plan();
 };
 
@@ -85,7 +90,7 @@ void unregister_plan(const void* key);
 // ------------------------------------------------------------- streams/timing
 
 cudaStream_t engine_stream();   // one non-blocking stream per host thread and device
-int grid_for(const void* kernel, int ntiles);
+int grid_for(const void* kernel, int ntiles, int dynamic_smem = 0);
 
 struct TimingState {
     int level = 0;
@@ -172,63 +177,250 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // --------------------------------------------------- fused tiled SpMV kernel
 //
-// One block walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... For each tile
-// it stages val[p] * v[idx[p]] for the tile's nonzeros in shared memory
-// (coalesced val/idx streams, gathers of v from L2), then reduces rows:
-//   rows of <= kShortRow entries: one thread, sequential sum from 0.0 in
-//     stored order (the exact rounding of a serial CPU loop),
-//   longer rows in a tile: one warp, lane-strided partials + xor tree,
-//   a row longer than kTileNnz: the whole block, strided partials + fixed tree.
-// Epi::row(r, sum, acc) consumes every row exactly once; Epi::finish reduces
-// the per-thread accumulators of reducing epilogues.
+// Warp-granular: every warp of a persistent grid walks warp chunks
+// gw, gw + total_warps, ... independently (no block-wide barrier on the path).
+// Each warp owns a double-buffered shared-memory slice. Lane 0 brings a chunk's
+// values and column indices in with two 1-D TMA bulk copies (cp.async.bulk,
+// completion counted on the slice's mbarrier), issued one chunk ahead, so the
+// HBM latency of the matrix stream overlaps the work on the current chunk:
+//   1. lane l owns row r0 + l and prefetches that row's epilogue data
+//      (Epi::load: y, bounds, steps, ...);
+//   2. lane l takes column indices p0 + l + 32 k (k < 8) from shared memory and
+//      issues its gathers v[idx] back to back (the vectors stay L2-resident),
+//      then overwrites each value slot with val[p] * v[idx[p]];
+//   3. rows of at most kShortRow entries are summed by their owning lane
+//      sequentially in stored order from 0.0 (the exact rounding of a serial
+//      CPU loop), longer rows by the whole warp (lane-strided partials, xor tree);
+//   4. Epi::store / Epi::row finishes the PDHG step for the row.
+// A row longer than kChunkNnz is a chunk of its own, streamed from global memory
+// by the warp. The copies cover the 16-byte-aligned interior of the chunk
+// ([p0 rounded down, p1 rounded down) to 2 doubles / 4 ints); the at most 1 value
+// and 3 indices past the last aligned boundary are read with plain loads, so no
+// copy leaves the arrays. Waits are bounded: a wait that gives up counts in A.err
+// and the warp stops after draining its copies. Reducing epilogues keep per-thread
+// accumulators; Epi::finish combines them per block in a fixed order.
+
+constexpr int kStageVal = kChunkNnz + 2;  // doubles per buffer
+constexpr int kStageIdx = kChunkNnz + 4;  // ints per buffer
+struct WarpStage {
+    double val[2][kStageVal];
+    int idx[2][kStageIdx];
+    unsigned long long bar[2];
+};
+constexpr int kTiledSmem = kWarps * static_cast<int>(sizeof(WarpStage));
+constexpr long long kWaitLimit = 1ll << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    for (long long i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+struct Empty {};
+
+template <class E, class = void>
+struct HasLoad {
+    static constexpr bool value = false;
+};
+template <class E>
+struct HasLoad<E, decltype(void(&E::load))> {
+    static constexpr bool value = true;
+};
+
+template <class Epi, bool = HasLoad<Epi>::value>
+struct RowPre {
+    using type = Empty;
+    static __device__ __forceinline__ type load(const Epi&, int) { return {}; }
+    static __device__ __forceinline__ void apply(const Epi& e, int r, double s, const type&,
+                                                 typename Epi::Acc& acc) {
+        e.row(r, s, acc);
+    }
+};
+template <class Epi>
+struct RowPre<Epi, true> {
+    using type = typename Epi::Row;
+    static __device__ __forceinline__ type load(const Epi& e, int r) { return e.load(r); }
+    static __device__ __forceinline__ void apply(const Epi& e, int r, double s, const type& pre,
+                                                 typename Epi::Acc& acc) {
+        e.store(r, s, pre, acc);
+    }
+};
+
+struct Chunk {
+    int r0, r1, p0, p1, a0v, a1v, a0i, a1i;
+    __device__ __forceinline__ bool streamed() const { return p1 - p0 > kChunkNnz; }
+};
+
+__device__ __forceinline__ Chunk chunk_at(const TileCsr& A, int t) {
+    const int2 b0 = __ldg(A.tile + t), b1 = __ldg(A.tile + t + 1);
+    Chunk c;
+    c.r0 = b0.x;
+    c.r1 = b1.x;
+    c.p0 = b0.y;
+    c.p1 = b1.y;
+    c.a0v = c.p0 & ~1;
+    c.a1v = max(c.a0v, c.p1 & ~1);
+    c.a0i = c.p0 & ~3;
+    c.a1i = max(c.a0i, c.p1 & ~3);
+    return c;
+}
+
+// Lane 0: both bulk copies of a staged chunk into buffer b of the warp's slice.
+__device__ __forceinline__ void issue_chunk(const TileCsr& A, const Chunk& c, WarpStage& ws, int b) {
+    const unsigned vb = static_cast<unsigned>(c.a1v - c.a0v) * 8u;
+    const unsigned ib = static_cast<unsigned>(c.a1i - c.a0i) * 4u;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_arrive_expect(&ws.bar[b], vb + ib);
+    if (vb) bulk_load(ws.val[b], A.val + c.a0v, vb, &ws.bar[b]);
+    if (ib) bulk_load(ws.idx[b], A.idx + c.a0i, ib, &ws.bar[b]);
+}
 
 template <class Epi>
-__global__ void __launch_bounds__(kThreads) k_tiled(TileCsr A, const double* __restrict__ v, Epi epi) {
-    __shared__ double prod[kTileNnz];
+__global__ void __launch_bounds__(kThreads, 4) k_tiled(TileCsr A, const double* __restrict__ v, Epi epi) {
+    using P = RowPre<Epi>;
+    extern __shared__ __align__(16) unsigned char dyn[];
     __shared__ double red[kWarps * 8];
     typename Epi::Acc acc;
     acc.init();
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
-        const int r0 = A.tile_row[t], r1 = A.tile_row[t + 1];
-        const int p0 = __ldg(A.ptr + r0), p1 = __ldg(A.ptr + r1);
-        if (p1 - p0 > kTileNnz) {
-            double s = 0.0;
-            for (int p = p0 + tid; p < p1; p += kThreads)
-                s += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
-            s = warp_sum(s);
-            if (lane == 0) red[warp] = s;
-            __syncthreads();
-            if (tid == 0) {
-                double total = red[0];
-                for (int w = 1; w < kWarps; ++w) total += red[w];
-                epi.row(r0, total, acc);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpStage& ws = reinterpret_cast<WarpStage*>(dyn)[warp];
+    const int nw = gridDim.x * kWarps;
+    const unsigned full = 0xffffffffu;
+    if (lane == 0) {
+        mbar_init(&ws.bar[0], 1);
+        mbar_init(&ws.bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    unsigned phase = 0;   // bit b: parity to wait for on buffer b
+    unsigned pending = 0; // bit b: a copy into buffer b is in flight
+    bool aborted = false;
+    int t = blockIdx.x * kWarps + warp;
+    Chunk cur{};
+    if (t < A.ntiles) {
+        cur = chunk_at(A, t);
+        if (!cur.streamed()) {
+            if (lane == 0) issue_chunk(A, cur, ws, 0);
+            pending |= 1u;
+        }
+    }
+    for (int k = 0; t < A.ntiles; ++k, t += nw) {
+        const int b = k & 1;
+        const int tn = t + nw;
+        Chunk nxt{};
+        if (tn < A.ntiles) {
+            nxt = chunk_at(A, tn);
+            if (!nxt.streamed()) {
+                if (lane == 0) issue_chunk(A, nxt, ws, b ^ 1);
+                pending |= 2u >> b;  // bit (b ^ 1)
             }
-            __syncthreads();
+        }
+        const int my = cur.r0 + lane;
+        const bool owns = my < cur.r1;
+        typename P::type pre{};
+        int q0 = 0, q1 = 0;
+        if (owns) {
+            pre = P::load(epi, my);
+            q0 = __ldg(A.ptr + my) - cur.a0v;
+            q1 = __ldg(A.ptr + my + 1) - cur.a0v;
+        }
+        if (cur.streamed()) {
+            double s0 = 0.0, s1 = 0.0;
+            int p = cur.p0 + lane;
+            for (; p + 32 < cur.p1; p += 64) {
+                s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
+                s1 += __ldcs(A.val + p + 32) * __ldg(v + __ldcs(A.idx + p + 32));
+            }
+            if (p < cur.p1) s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
+            const double s = warp_sum(s0 + s1);
+            if (lane == 0) P::apply(epi, cur.r0, s, pre, acc);
+            cur = nxt;
             continue;
         }
-#pragma unroll 4
-        for (int p = p0 + tid; p < p1; p += kThreads)
-            prod[p - p0] = dmul(__ldcs(A.val + p), __ldg(v + __ldcs(A.idx + p)));
-        __syncthreads();
-        for (int r = r0 + tid; r < r1; r += kThreads) {
-            const int q0 = __ldg(A.ptr + r) - p0, q1 = __ldg(A.ptr + r + 1) - p0;
-            if (q1 - q0 <= kShortRow) {
-                double s = 0.0;
-                for (int q = q0; q < q1; ++q) s = dadd(s, prod[q]);
-                epi.row(r, s, acc);
+        const bool ok = mbar_wait(&ws.bar[b], (phase >> b) & 1u);
+        phase ^= 1u << b;
+        pending &= ~(1u << b);
+        if (!__all_sync(full, ok)) {
+            if (lane == 0 && A.err) atomicAdd(A.err, 1u);
+            aborted = true;
+            break;
+        }
+        double* sval = ws.val[b];
+        const int* sidx = ws.idx[b];
+        int col[kPerLane];
+        double g[kPerLane];
+#pragma unroll
+        for (int e = 0; e < kPerLane; ++e) {
+            const int p = cur.p0 + 32 * e + lane;
+            col[e] = 0;
+            if (p < cur.p1) col[e] = p < cur.a1i ? sidx[p - cur.a0i] : __ldg(A.idx + p);
+        }
+#pragma unroll
+        for (int e = 0; e < kPerLane; ++e)
+            g[e] = cur.p0 + 32 * e + lane < cur.p1 ? __ldg(v + col[e]) : 0.0;
+#pragma unroll
+        for (int e = 0; e < kPerLane; ++e) {
+            const int p = cur.p0 + 32 * e + lane;
+            if (p < cur.p1) {
+                const double a = p < cur.a1v ? sval[p - cur.a0v] : __ldg(A.val + p);
+                sval[p - cur.a0v] = dmul(a, g[e]);
             }
         }
-        for (int r = r0 + warp; r < r1; r += kWarps) {
-            const int q0 = __ldg(A.ptr + r) - p0, q1 = __ldg(A.ptr + r + 1) - p0;
-            if (q1 - q0 > kShortRow) {
-                double s = 0.0;
-                for (int q = q0 + lane; q < q1; q += 32) s += prod[q];
-                s = warp_sum(s);
-                if (lane == 0) epi.row(r, s, acc);
-            }
+        __syncwarp();
+        const int len = q1 - q0;
+        if (owns && len <= kShortRow) {
+            double s = 0.0;
+            for (int q = q0; q < q1; ++q) s = dadd(s, sval[q]);
+            P::apply(epi, my, s, pre, acc);
         }
-        __syncthreads();
+        unsigned long_rows = __ballot_sync(full, owns && len > kShortRow);
+        while (long_rows) {
+            const int l = __ffs(long_rows) - 1;
+            long_rows &= long_rows - 1;
+            const int lq0 = __shfl_sync(full, q0, l), lq1 = __shfl_sync(full, q1, l);
+            double s = 0.0;
+            for (int q = lq0 + lane; q < lq1; q += 32) s += sval[q];
+            s = warp_sum(s);
+            if (lane == l) P::apply(epi, my, s, pre, acc);
+        }
+        __syncwarp();
+        cur = nxt;
+    }
+    if (aborted && lane == 0) {
+        // drain copies still in flight before the slice is released
+        for (int b = 0; b < 2; ++b)
+            if (pending & (1u << b)) mbar_wait(&ws.bar[b], (phase >> b) & 1u);
     }
     epi.finish(acc, red);
 }
@@ -242,16 +434,17 @@ struct StoreEpi {
 };
 
 template <class Epi>
-inline int launch_tiled(const TileCsr& A, const double* v, const Epi& epi, cudaStream_t stream,
-                        int grid) {
-    if (A.ntiles == 0) return 0;
-    k_tiled<Epi><<<grid, kThreads, 0, stream>>>(A, v, epi);
-    return 0;
+inline int tiled_grid(const TileCsr& A) {
+    const void* k = reinterpret_cast<const void*>(&k_tiled<Epi>);
+    return grid_for(k, (A.ntiles + kWarps - 1) / kWarps, kTiledSmem);
 }
 
 template <class Epi>
-inline int tiled_grid(const TileCsr& A) {
-    return grid_for(reinterpret_cast<const void*>(&k_tiled<Epi>), A.ntiles);
+inline int launch_tiled(const TileCsr& A, const double* v, const Epi& epi, cudaStream_t stream,
+                        int grid) {
+    if (A.ntiles == 0) return 0;
+    k_tiled<Epi><<<grid, kThreads, kTiledSmem, stream>>>(A, v, epi);
+    return 0;
 }
 
 // Final fixed-order combine of per-block partials: out[k] = op_g partial[g*NS+k].

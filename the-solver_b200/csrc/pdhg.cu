@@ -22,6 +22,7 @@
 #include <climits>
 #include <limits>
 #include <map>
+#include <tuple>
 
 namespace b200 {
 
@@ -36,10 +37,13 @@ struct DualCudaEpi {
     double sigma;
     double* __restrict__ y_new;
     using Acc = NoAcc;
-    __device__ __forceinline__ void row(int i, double act, Acc&) const {
-        const double s = sig ? sig[i] : sigma;
-        const double trial = dadd(y[i], dmul(s, act));
-        y_new[i] = dsub(trial, dmul(s, box_ieee(ddiv(trial, s), rl[i], ru[i])));
+    struct Row {
+        double y, lo, hi, s;
+    };
+    __device__ __forceinline__ Row load(int i) const { return Row{y[i], rl[i], ru[i], sig ? sig[i] : sigma}; }
+    __device__ __forceinline__ void store(int i, double act, const Row& r, Acc&) const {
+        const double trial = dadd(r.y, dmul(r.s, act));
+        y_new[i] = dsub(trial, dmul(r.s, box_ieee(ddiv(trial, r.s), r.lo, r.hi)));
     }
     __device__ __forceinline__ void finish(Acc&, double*) const {}
 };
@@ -57,15 +61,17 @@ struct PrimalCudaEpi {
     double* __restrict__ x_new;
     double* __restrict__ x_bar;
     using Acc = NoAcc;
-    __device__ __forceinline__ void row(int j, double g, Acc&) const {
-        const double t = tauv ? tauv[j] : tau;
-        const double curvature = qdiag ? qdiag[j] : 0.0;
-        const double qg = qgrad ? qgrad[j] : 0.0;
-        const double xj = x[j];
-        const double trial = ddiv(dsub(xj, dmul(t, dadd(dadd(c[j], g), qg))), dadd(1.0, dmul(t, curvature)));
-        const double next = box_ieee(trial, cl[j], cu[j]);
+    struct Row {
+        double x, c, t, lo, hi, curvature, qg;
+    };
+    __device__ __forceinline__ Row load(int j) const {
+        return Row{x[j], c[j], tauv ? tauv[j] : tau, cl[j], cu[j], qdiag ? qdiag[j] : 0.0, qgrad ? qgrad[j] : 0.0};
+    }
+    __device__ __forceinline__ void store(int j, double g, const Row& r, Acc&) const {
+        const double trial = ddiv(dsub(r.x, dmul(r.t, dadd(dadd(r.c, g), r.qg))), dadd(1.0, dmul(r.t, r.curvature)));
+        const double next = box_ieee(trial, r.lo, r.hi);
         x_new[j] = next;
-        x_bar[j] = dadd(next, dmul(theta, dsub(next, xj)));
+        x_bar[j] = dadd(next, dmul(theta, dsub(next, r.x)));
     }
     __device__ __forceinline__ void finish(Acc&, double*) const {}
 };
@@ -79,13 +85,15 @@ struct DualSkEpi {
     double* __restrict__ y_new;
     double* __restrict__ partial;
     using Acc = Slots<1, 0u>;
-    __device__ __forceinline__ void row(int i, double act, Acc& acc) const {
-        const double s = sig[i];
-        const double yi = y[i];
-        const double trial = dadd(yi, dmul(s, act));
-        const double yn = dsub(trial, dmul(s, box_sk(ddiv(trial, s), rl[i], ru[i])));
+    struct Row {
+        double y, lo, hi, s;
+    };
+    __device__ __forceinline__ Row load(int i) const { return Row{y[i], rl[i], ru[i], sig[i]}; }
+    __device__ __forceinline__ void store(int i, double act, const Row& r, Acc& acc) const {
+        const double trial = dadd(r.y, dmul(r.s, act));
+        const double yn = dsub(trial, dmul(r.s, box_sk(ddiv(trial, r.s), r.lo, r.hi)));
         y_new[i] = yn;
-        acc.max(0, fabs(dsub(yn, yi)));
+        acc.max(0, fabs(dsub(yn, r.y)));
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
 };
@@ -102,18 +110,22 @@ struct PrimalSkEpi {
     double* __restrict__ x_new;
     double* __restrict__ x_bar;
     using Acc = NoAcc;
-    __device__ __forceinline__ void row(int j, double g, Acc&) const {
-        const double t = tauv[j];
-        const double xj = x[j];
+    struct Row {
+        double x, c, t, lo, hi, qd, qx;
+    };
+    __device__ __forceinline__ Row load(int j) const {
+        return Row{x[j], c[j], tauv[j], cl[j], cu[j], qdiag ? qdiag[j] : 0.0, qx ? qx[j] : 0.0};
+    }
+    __device__ __forceinline__ void store(int j, double g, const Row& r, Acc&) const {
         double xn;
         if (qdiag) {
-            xn = ddiv(dsub(xj, dmul(t, dadd(c[j], g))), dadd(1.0, dmul(t, qdiag[j])));
+            xn = ddiv(dsub(r.x, dmul(r.t, dadd(r.c, g))), dadd(1.0, dmul(r.t, r.qd)));
         } else {
-            xn = dsub(xj, dmul(t, dadd(dadd(c[j], qx ? qx[j] : 0.0), g)));
+            xn = dsub(r.x, dmul(r.t, dadd(dadd(r.c, r.qx), g)));
         }
-        xn = box_sk(xn, cl[j], cu[j]);
+        xn = box_sk(xn, r.lo, r.hi);
         x_new[j] = xn;
-        x_bar[j] = dsub(dmul(2.0, xn), xj);
+        x_bar[j] = dsub(dmul(2.0, xn), r.x);
     }
     __device__ __forceinline__ void finish(Acc&, double*) const {}
 };
@@ -283,6 +295,32 @@ __global__ void k_sk_step_scale(const double* __restrict__ x, const double* __re
     block_store(acc, partial, smem);
 }
 
+// Per-element input checks of cuda/src/sankhya_cuda_lp.cu:136-153 on the
+// uploaded arrays; failure classes are or-ed into *flags (1 cost / column bound,
+// 2 row bound, 4 primal step, 8 dual step, 16 quadratic diagonal).
+__device__ __forceinline__ bool dev_valid_lower(double v) { return !isnan(v) && !(isinf(v) && v > 0.0); }
+__device__ __forceinline__ bool dev_valid_upper(double v) { return !isnan(v) && !(isinf(v) && v < 0.0); }
+
+__global__ void k_validate_fixed(int n, int m, const double* __restrict__ c, const double* __restrict__ cl,
+                                 const double* __restrict__ cu, const double* __restrict__ rl,
+                                 const double* __restrict__ ru, const double* __restrict__ tauv,
+                                 const double* __restrict__ sigv, const double* __restrict__ qd,
+                                 unsigned int* __restrict__ flags) {
+    unsigned int f = 0;
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        if (!isfinite(c[j]) || !dev_valid_lower(cl[j]) || !dev_valid_upper(cu[j]) || cl[j] > cu[j]) f |= 1u;
+        if (tauv && (!isfinite(tauv[j]) || tauv[j] <= 0.0)) f |= 4u;
+        if (qd && (!isfinite(qd[j]) || qd[j] < 0.0)) f |= 16u;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        if (!dev_valid_lower(rl[i]) || !dev_valid_upper(ru[i]) || rl[i] > ru[i]) f |= 2u;
+        if (sigv && (!isfinite(sigv[i]) || sigv[i] <= 0.0)) f |= 8u;
+    }
+    f = __reduce_or_sync(0xffffffffu, f);
+    if ((threadIdx.x & 31) == 0 && f) atomicOr(flags, f);
+}
+
 // Q x for a diagonal Q (sk_solve.c:909: qx_j = qdiag_j x_j).
 __global__ void k_diag_mul(const double* __restrict__ qd, const double* __restrict__ xv, double* __restrict__ out,
                            int n) {
@@ -319,6 +357,7 @@ struct Workspace {
     double *x[2] = {nullptr, nullptr}, *y[2] = {nullptr, nullptr};
     double *x_bar = nullptr, *qx = nullptr, *x_prev = nullptr, *act = nullptr;
     double *part_a = nullptr, *part_b = nullptr, *part_c = nullptr, *out = nullptr;
+    unsigned int* flags = nullptr;
     int n = 0, m = 0;
 
     int allocate(int n_, int m_, int max_grid) {
@@ -327,7 +366,7 @@ struct Workspace {
         const size_t nb = (static_cast<size_t>(n) * 8 + 255) / 256 * 256;
         const size_t mb = (static_cast<size_t>(m) * 8 + 255) / 256 * 256;
         const size_t pb = (static_cast<size_t>(max_grid) * 8 * 8 + 255) / 256 * 256;
-        const size_t total = 11 * nb + 6 * mb + 3 * pb + 256;
+        const size_t total = 11 * nb + 6 * mb + 3 * pb + 512;
         if (blob.alloc(total, "cudaMalloc PDHG workspace")) return -1;
         char* p = blob.as<char>();
         auto take = [&](size_t b) { double* r = reinterpret_cast<double*>(p); p += b; return r; };
@@ -336,9 +375,19 @@ struct Workspace {
         take(nb);
         rl = take(mb); ru = take(mb); sigv = take(mb); y[0] = take(mb); y[1] = take(mb); act = take(mb);
         part_a = take(pb); part_b = take(pb); part_c = take(pb); out = take(256);
+        flags = reinterpret_cast<unsigned int*>(take(256));
         return 0;
     }
 };
+
+// True when a bounded device wait of this plan's launches gave up (the word is
+// then cleared so the next call starts clean).
+static bool wait_timed_out(const Plan& plan) {
+    unsigned int word = 0;
+    if (!plan.d_err || cudaMemcpy(&word, plan.d_err, sizeof(word), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    if (word) cudaMemset(plan.d_err, 0, sizeof(word));
+    return word != 0;
+}
 
 // A host-visible pinned slot for checkpoint results, one per thread.
 static double* pinned_out() {
@@ -350,6 +399,36 @@ static double* pinned_out() {
     if (!h.p && cudaMallocHost(reinterpret_cast<void**>(&h.p), 64 * sizeof(double)) != cudaSuccess) h.p = nullptr;
     return h.p;
 }
+
+// Captured iteration graphs, keyed by everything a captured launch bakes in.
+struct GraphKey {
+    cudaStream_t stream;
+    const void* q;
+    int has_qdiag, has_steps, chunk, parity, sem;
+    double tau, sigma, theta;
+    bool operator<(const GraphKey& o) const {
+        return std::tie(stream, q, has_qdiag, has_steps, chunk, parity, sem, tau, sigma, theta) <
+               std::tie(o.stream, o.q, o.has_qdiag, o.has_steps, o.chunk, o.parity, o.sem, o.tau, o.sigma, o.theta);
+    }
+};
+
+struct GraphMap {
+    std::map<GraphKey, cudaGraphExec_t> map;
+    GraphMap() = default;
+    GraphMap(const GraphMap&) = delete;
+    GraphMap& operator=(const GraphMap&) = delete;
+    ~GraphMap() {
+        for (auto& kv : map)
+            if (kv.second) cudaGraphExecDestroy(kv.second);
+    }
+};
+
+// Per-plan cache of the fixed-step solver's device state: a later call with
+// the same shape reuses the workspace and the graphs captured over it.
+struct FixedCache {
+    Workspace w;
+    GraphMap graphs;
+};
 
 struct Solver {
     Sem sem;
@@ -363,13 +442,8 @@ struct Solver {
     int cur = 0;
     int grid_dual = 1, grid_primal = 1, grid_q = 1;
     int launches = 0;
-    // graph cache: (iterations, parity) -> exec
-    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
-
-    ~Solver() {
-        for (auto& kv : graphs)
-            if (kv.second) cudaGraphExecDestroy(kv.second);
-    }
+    GraphMap local_graphs;
+    GraphMap* graphs = &local_graphs;
 
     void setup_grids() {
         if (sem == Sem::Cuda) {
@@ -438,9 +512,10 @@ struct Solver {
         }
         while (k > 0) {
             const int chunk = k > 64 ? 64 : k;
-            auto key = std::make_pair(chunk, cur);
-            auto it = graphs.find(key);
-            if (it == graphs.end()) {
+            const GraphKey key{stream, Q, has_qdiag ? 1 : 0, has_steps ? 1 : 0, chunk, cur, static_cast<int>(sem),
+                               tau, sigma, theta};
+            auto it = graphs->map.find(key);
+            if (it == graphs->map.end()) {
                 const int saved_cur = cur, saved_launches = launches;
                 cudaGraph_t g;
                 B200_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -450,7 +525,7 @@ struct Solver {
                 cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
                 cudaGraphDestroy(g);
                 if (e != cudaSuccess) return fail_cuda("graph instantiate", e);
-                it = graphs.emplace(key, exec).first;
+                it = graphs->map.emplace(key, exec).first;
                 cur = saved_cur;
                 launches = saved_launches;
             }
@@ -467,8 +542,6 @@ static double now_seconds() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-static bool valid_lower(double v) { return !std::isnan(v) && !(std::isinf(v) && v > 0.0); }
-static bool valid_upper(double v) { return !std::isnan(v) && !(std::isinf(v) && v < 0.0); }
 
 struct EventTimer {
     cudaEvent_t a = nullptr, b = nullptr;
@@ -519,22 +592,10 @@ static int solve_fixed(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessi
     if (pstep == nullptr && (s.tau <= 0.0 || s.sigma <= 0.0)) return fail_msg("non-positive scalar step");
     const int rows = matrix->rows, cols = matrix->cols;
     if (rows < 0 || cols < 0) return fail_msg("negative dimension");
-    for (int j = 0; j < cols; ++j)
-        if (!std::isfinite(c[j]) || !valid_lower(cl[j]) || !valid_upper(cu[j]) || cl[j] > cu[j])
-            return fail_msg("invalid cost or column bound");
-    for (int i = 0; i < rows; ++i)
-        if (!valid_lower(rl[i]) || !valid_upper(ru[i]) || rl[i] > ru[i]) return fail_msg("invalid row bound");
-    if (pstep != nullptr) {
-        for (int j = 0; j < cols; ++j)
-            if (!std::isfinite(pstep[j]) || pstep[j] <= 0.0) return fail_msg("invalid primal step");
-        for (int i = 0; i < rows; ++i)
-            if (!std::isfinite(dstep[i]) || dstep[i] <= 0.0) return fail_msg("invalid dual step");
-    }
     if (hessian != nullptr && (qdiag != nullptr || hessian->rows != cols || hessian->cols != cols))
         return fail_msg("invalid Hessian");
-    if (qdiag != nullptr)
-        for (int j = 0; j < cols; ++j)
-            if (!std::isfinite(qdiag[j]) || qdiag[j] < 0.0) return fail_msg("invalid quadratic diagonal");
+    // The per-element checks of sankhya_cuda_lp.cu:136-153 run on the device
+    // right after the upload (k_validate_fixed), before any iteration.
 
     std::shared_ptr<Plan> plan, qplan;
     if (get_plan(matrix, &plan)) return -1;
@@ -546,9 +607,22 @@ static int solve_fixed(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessi
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan->device);
 
-    Workspace local;
-    Workspace* w = &local;
-    if (w->allocate(cols, rows, sms * 8)) return -1;
+    // The plan's cached workspace and graphs, unless another thread holds them.
+    std::unique_lock<std::mutex> lock(plan->workspace_mutex, std::try_to_lock);
+    std::shared_ptr<FixedCache> cache;
+    if (lock.owns_lock()) {
+        cache = std::static_pointer_cast<FixedCache>(plan->solve_cache);
+        if (!cache || cache->w.n != cols || cache->w.m != rows) {
+            plan->solve_cache.reset();
+            cache = std::make_shared<FixedCache>();
+            if (cache->w.allocate(cols, rows, sms * 8)) return -1;
+            plan->solve_cache = cache;
+        }
+    } else {
+        cache = std::make_shared<FixedCache>();
+        if (cache->w.allocate(cols, rows, sms * 8)) return -1;
+    }
+    Workspace* w = &cache->w;
 
     const size_t nb = sizeof(double) * static_cast<size_t>(cols), mb = sizeof(double) * static_cast<size_t>(rows);
     EventTimer t_h2d(timed, stream);
@@ -566,7 +640,22 @@ static int solve_fixed(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessi
         B200_TRY(cudaMemsetAsync(w->y[0], 0, mb, stream), "zero y");
     }
     if (cols > 0) k_init_box_ieee<<<elem_grid(cols), kThreads, 0, stream>>>(cols, w->cl, w->cu, w->x[0], w->x_bar);
+    B200_TRY(cudaMemsetAsync(w->flags, 0, sizeof(unsigned int), stream), "clear flags");
+    k_validate_fixed<<<elem_grid(std::max(rows, cols)), kThreads, 0, stream>>>(
+        cols, rows, w->c, w->cl, w->cu, w->rl, w->ru, pstep ? w->tauv : nullptr, dstep ? w->sigv : nullptr,
+        qdiag ? w->qdiag : nullptr, w->flags);
     B200_TRY(cudaGetLastError(), "init launch");
+    {
+        unsigned int* hflags = reinterpret_cast<unsigned int*>(pinned_out() + 48);
+        B200_TRY(cudaMemcpyAsync(hflags, w->flags, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream), "flags");
+        B200_TRY(cudaStreamSynchronize(stream), "validation");
+        const unsigned int f = *hflags;
+        if (f & 1u) return fail_msg("invalid cost or column bound");
+        if (f & 2u) return fail_msg("invalid row bound");
+        if (f & 4u) return fail_msg("invalid primal step");
+        if (f & 8u) return fail_msg("invalid dual step");
+        if (f & 16u) return fail_msg("invalid quadratic diagonal");
+    }
     ts.last.h2d_ms = t_h2d.stop();
 
     Solver sv;
@@ -576,6 +665,8 @@ static int solve_fixed(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessi
     sv.AT = &plan->at;
     sv.Q = qplan ? &qplan->a : nullptr;
     sv.w = w;
+    // graphs over an explicit Hessian bake in that matrix's pointers: keep them per call
+    sv.graphs = hessian == nullptr ? &cache->graphs : &sv.local_graphs;
     sv.has_qdiag = qdiag != nullptr;
     sv.has_steps = pstep != nullptr;
     sv.tau = s.tau;
@@ -622,6 +713,7 @@ static int solve_fixed(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessi
         B200_TRY(cudaStreamSynchronize(stream), "checkpoint");
         ts.last.checkpoint_ms += t_chk.stop();
         ts.last.checkpoints += 1;
+        if (wait_timed_out(*plan)) return fail_msg("device wait for a tile copy gave up");
         const double nonfinite = std::max(host[0], host[8]);
         const double objective = host[9];
         if (nonfinite > 0.0 || !std::isfinite(objective)) {
@@ -711,10 +803,10 @@ struct OwnedPair {
         B200_TRY(cudaMemcpy(tiles.p, ta.data(), tiles.bytes, cudaMemcpyHostToDevice), "upload tiles");
         B200_TRY(cudaMemcpy(tptr.p, tp, tptr.bytes, cudaMemcpyHostToDevice), "upload A^T");
         B200_TRY(cudaMemcpy(ttiles.p, tb.data(), ttiles.bytes, cudaMemcpyHostToDevice), "upload tiles");
-        a = TileCsr{rows, cols, nnz, static_cast<int>(ta.size()) - 1, ptr.as<int>(), idx.as<int>(), val.as<double>(),
-                    tiles.as<int>()};
-        at = TileCsr{cols, rows, nnz, static_cast<int>(tb.size()) - 1, tptr.as<int>(), tidx.as<int>(), tval.as<double>(),
-                     ttiles.as<int>()};
+        a = TileCsr{rows, cols, nnz, static_cast<int>(ta.size()) / 2 - 1, ptr.as<int>(), idx.as<int>(),
+                    val.as<double>(), tiles.as<int2>()};
+        at = TileCsr{cols, rows, nnz, static_cast<int>(tb.size()) / 2 - 1, tptr.as<int>(), tidx.as<int>(),
+                     tval.as<double>(), ttiles.as<int2>()};
         return 0;
     }
 };

@@ -101,12 +101,15 @@ struct PrimalCandEpi {
     double* __restrict__ x_cand;
     double* __restrict__ partial;
     using Acc = Slots<1, 1u>;
-    __device__ __forceinline__ void row(int j, double aty, Acc& acc) const {
+    struct Row {
+        double x, c, lo, hi;
+    };
+    __device__ __forceinline__ Row load(int j) const { return Row{x[j], c[j], cl[j], cu[j]}; }
+    __device__ __forceinline__ void store(int j, double aty, const Row& r, Acc& acc) const {
         const double tau = st->eta / st->omega;
-        const double xj = x[j];
-        const double xc = clampf(xj - tau * (c[j] + aty), cl[j], cu[j]);
+        const double xc = clampf(r.x - tau * (r.c + aty), r.lo, r.hi);
         x_cand[j] = xc;
-        const double dx = xc - xj;
+        const double dx = xc - r.x;
         acc.add(0, dx * dx);
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
@@ -123,11 +126,15 @@ struct ProbeEpi {
     const double* __restrict__ partial_dx;  // K2's [grid_dx]
     int grid_dx;
     using Acc = Slots<2, 3u>;
-    __device__ __forceinline__ void row(int i, double axc, Acc& acc) const {
+    struct Row {
+        double y, yc, ax;
+    };
+    __device__ __forceinline__ Row load(int i) const { return Row{y[i], y_cand[i], ax[i]}; }
+    __device__ __forceinline__ void store(int i, double axc, const Row& r, Acc& acc) const {
         ax_cand[i] = axc;
-        const double dy = y_cand[i] - y[i];
+        const double dy = r.yc - r.y;
         acc.add(0, dy * dy);
-        acc.add(1, dy * (axc - ax[i]));
+        acc.add(1, dy * (axc - r.ax));
     }
     __device__ void finish(Acc& acc, double* smem) const {
         block_store(acc, partial, smem);
@@ -409,7 +416,7 @@ __global__ void k_normalize(double* __restrict__ v, int n, const double* __restr
 //                       out[r] = min, out2[r] = max of |val| rs cs     (mode 2, geometric passes)
 __global__ void k_row_stats(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
                             const double* __restrict__ val, const double* __restrict__ rs,
-                            const double* __restrict__ cs, int mode, double* __restrict__ out,
+                            const double* __restrict__ cs, int mode, int transposed, double* __restrict__ out,
                             double* __restrict__ out2) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -424,7 +431,8 @@ __global__ void k_row_stats(int rows, const int* __restrict__ ptr, const int* __
                 const double v = fabs(val[p]);
                 if (v != 0.0) a += v * rsr * cs[idx[p]];
             } else {
-                const double v = fabs(val[p]) * rsr * cs[idx[p]];
+                // (|a| R_i) C_j in both orientations, as sk_scale.c:41 and :52 form it
+                const double v = transposed ? fabs(val[p]) * cs[idx[p]] * rsr : fabs(val[p]) * rsr * cs[idx[p]];
                 if (v > 0.0) { a = fmin(a, v); b = fmax(b, v); }
             }
         }
@@ -634,10 +642,10 @@ struct PdlpRun {
             if (mode & SANKHYA_B200_SCALE_POW2) {
                 for (int pass = 0; pass < 4; ++pass) {
                     // columns first (sk_scale.c:38-47), then rows (:48-57)
-                    k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 2,
+                    k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 2, 1,
                                                                tmp_n, x_avg);
                     k_geo_update<<<gn, kThreads, 0, stream>>>(Cs, tmp_n, x_avg, n);
-                    k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 2,
+                    k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 2, 0,
                                                                tmp_m, y_avg);
                     k_geo_update<<<gm, kThreads, 0, stream>>>(R, tmp_m, y_avg, m);
                     launches += 4;
@@ -649,9 +657,9 @@ struct PdlpRun {
                 // factors accumulate in (R, Cs); identity restored if not converged
                 bool converged = false;
                 for (int it = 0; it < ruiz_iters; ++it) {
-                    k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 0,
+                    k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 0, 0,
                                                                tmp_m, nullptr);
-                    k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 0,
+                    k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 0, 1,
                                                                tmp_n, nullptr);
                     const int g = std::min(eg(m + n), sms * 4);
                     k_ruiz_dev<<<g, kThreads, 0, stream>>>(tmp_m, m, tmp_n, n, part_a);
@@ -670,9 +678,9 @@ struct PdlpRun {
                 }
             }
             if (mode & SANKHYA_B200_SCALE_POCK_CHAMBOLLE) {
-                k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 1, tmp_m,
+                k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 1, 0, tmp_m,
                                                            nullptr);
-                k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 1, tmp_n,
+                k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 1, 1, tmp_n,
                                                            nullptr);
                 k_inv_sqrt_or_one<<<gm, kThreads, 0, stream>>>(tmp2_m, tmp_m, m);
                 k_inv_sqrt_or_one<<<gn, kThreads, 0, stream>>>(x_avg, tmp_n, n);
@@ -918,6 +926,14 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         if (run.window(period, adaptive, tau, sigma, slot)) return -1;
         B200_TRY(cudaStreamSynchronize(stream), "PDLP window");
         ++syncs;
+        {
+            unsigned int word = 0;
+            if (plan->d_err && cudaMemcpy(&word, plan->d_err, sizeof(word), cudaMemcpyDeviceToHost) == cudaSuccess &&
+                word != 0) {
+                cudaMemset(plan->d_err, 0, sizeof(word));
+                return fail_msg("device wait for a tile copy gave up");
+            }
+        }
         iteration += period;
         iterations_since_restart += period;
         ++windows_since_restart;
@@ -992,4 +1008,35 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     ts.last.checkpoints = syncs;
     ts.last.kernel_launches = run.launches;
     return numeric ? -2 : 0;
+}
+
+extern "C" int sankhya_b200_scale_factors(const SankhyaCudaCSR* matrix, int scaling, int ruiz_iterations,
+                                          double ruiz_tolerance, double* row_scale, double* col_scale) {
+    clear_error();
+    (void)cudaGetLastError();
+    if (!matrix || (matrix->rows > 0 && !row_scale) || (matrix->cols > 0 && !col_scale) || ruiz_iterations < 0 ||
+        !(ruiz_tolerance > 0.0) || (scaling & ~7))
+        return fail_msg("invalid scaling arguments");
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) return fail_msg("no CUDA device available");
+    std::shared_ptr<Plan> plan;
+    if (get_plan(matrix, &plan)) return -1;
+    PdlpRun run;
+    run.stream = engine_stream();
+    if (run.allocate(*plan)) return -1;
+    struct HostSlot {
+        double* p = nullptr;
+        ~HostSlot() { if (p) cudaFreeHost(p); }
+    } hs;
+    B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&hs.p), 64 * sizeof(double)), "cudaMallocHost");
+    run.host = hs.p;
+    const int n = matrix->cols, m = matrix->rows;
+    const size_t nb = sizeof(double) * static_cast<size_t>(n), mb = sizeof(double) * static_cast<size_t>(m);
+    B200_TRY(cudaMemsetAsync(run.blob.p, 0, run.blob.bytes, run.stream), "clear workspace");
+    int syncs = 0;
+    if (run.scale(*plan, scaling, ruiz_iterations, ruiz_tolerance, &syncs)) return -1;
+    if (n) B200_TRY(cudaMemcpyAsync(col_scale, run.Cs, nb, cudaMemcpyDeviceToHost, run.stream), "download C");
+    if (m) B200_TRY(cudaMemcpyAsync(row_scale, run.R, mb, cudaMemcpyDeviceToHost, run.stream), "download R");
+    B200_TRY(cudaStreamSynchronize(run.stream), "scaling");
+    return 0;
 }

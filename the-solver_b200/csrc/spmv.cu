@@ -100,8 +100,8 @@ extern "C" int sankhya_cuda_spmv_f64(int rows, int cols, int nnz, const int* row
     A.ptr = d_ptr.as<int>();
     A.idx = d_idx.as<int>();
     A.val = d_val.as<double>();
-    A.ntiles = static_cast<int>(tiles.size()) - 1;
-    A.tile_row = d_tiles.as<int>();
+    A.ntiles = static_cast<int>(tiles.size()) / 2 - 1;
+    A.tile = d_tiles.as<int2>();
     launch_tiled(A, d_x.as<double>(), StoreEpi{d_y.as<double>()}, 0, tiled_grid<StoreEpi>(A));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda("CSR SpMV launch", e);
