@@ -113,7 +113,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
+    """One process per GPU (torchrun env). Replicas only: the process group is
+    used for the barrier and the max-over-ranks of the timed region, never for
+    data."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -121,17 +124,25 @@ def dist_setup(n_gpus):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
+def _reduce_device():
+    import torch
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def barrier_max(value, world):
+    """Max of a per-rank scalar over all ranks (the job's time is the slowest rank's)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -140,6 +151,12 @@ def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def job_throughput(world, bytes_per_unit, units_per_rank, seconds_max):
+    """Whole-job rate: every rank processed units_per_rank units of bytes_per_unit
+    bytes; the job took the slowest rank's time."""
+    return world * bytes_per_unit * units_per_rank / seconds_max / 1e9
 
 
 def reference_loop_gbs(inst, iterations):
@@ -245,8 +262,8 @@ def run_engine(args, world, rank, local):
     wall = barrier_max(wall, world)
     dev_ms = barrier_max(dev_ms, world)
     bytes_iter = iteration_bytes(m, n, nnz)
-    value = world * bytes_iter * iters / (dev_ms / 1e3) / 1e9
-    e2e = world * bytes_iter * iters / wall / 1e9
+    value = job_throughput(world, bytes_iter, iters, dev_ms / 1e3)
+    e2e = job_throughput(world, bytes_iter, iters, wall)
     if rank != 0:
         return 0
     peak, peak_kind = measured_peak()

@@ -179,73 +179,23 @@ __device__ __forceinline__ double warp_sum(double v) {
 //
 // Warp-granular: every warp of a persistent grid walks warp chunks
 // gw, gw + total_warps, ... independently (no block-wide barrier on the path).
-// Each warp owns a double-buffered shared-memory slice. Lane 0 brings a chunk's
-// values and column indices in with two 1-D TMA bulk copies (cp.async.bulk,
-// completion counted on the slice's mbarrier), issued one chunk ahead, so the
-// HBM latency of the matrix stream overlaps the work on the current chunk:
+// For a chunk of rows [r0, r1) and nonzeros [p0, p1):
+//   0. lane 0 asks the TMA unit to pull the warp's NEXT chunk of values and
+//      column indices into L2 (cp.async.bulk.prefetch.L2, no shared memory, no
+//      completion to wait for), so that chunk's loads below hit L2, not HBM;
 //   1. lane l owns row r0 + l and prefetches that row's epilogue data
-//      (Epi::load: y, bounds, steps, ...);
-//   2. lane l takes column indices p0 + l + 32 k (k < 8) from shared memory and
-//      issues its gathers v[idx] back to back (the vectors stay L2-resident),
-//      then overwrites each value slot with val[p] * v[idx[p]];
-//   3. rows of at most kShortRow entries are summed by their owning lane
-//      sequentially in stored order from 0.0 (the exact rounding of a serial
-//      CPU loop), longer rows by the whole warp (lane-strided partials, xor tree);
+//      (Epi::load: y, bounds, steps, ...) into registers;
+//   2. lane l loads values and column indices p0 + l + 32 k (k < 8, coalesced,
+//      evict-first) and issues its 8 gathers v[idx] back to back (the vectors
+//      stay L2-resident);
+//   3. products go to the warp's 2 KB shared-memory slice; rows of at most
+//      kShortRow entries are summed by their owning lane sequentially in stored
+//      order from 0.0 (the exact rounding of a serial CPU loop), longer rows by
+//      the whole warp (lane-strided partials, xor tree);
 //   4. Epi::store / Epi::row finishes the PDHG step for the row.
-// A row longer than kChunkNnz is a chunk of its own, streamed from global memory
-// by the warp. The copies cover the 16-byte-aligned interior of the chunk
-// ([p0 rounded down, p1 rounded down) to 2 doubles / 4 ints); the at most 1 value
-// and 3 indices past the last aligned boundary are read with plain loads, so no
-// copy leaves the arrays. Waits are bounded: a wait that gives up counts in A.err
-// and the warp stops after draining its copies. Reducing epilogues keep per-thread
-// accumulators; Epi::finish combines them per block in a fixed order.
-
-constexpr int kStageVal = kChunkNnz + 2;  // doubles per buffer
-constexpr int kStageIdx = kChunkNnz + 4;  // ints per buffer
-struct WarpStage {
-    double val[2][kStageVal];
-    int idx[2][kStageIdx];
-    unsigned long long bar[2];
-};
-constexpr int kTiledSmem = kWarps * static_cast<int>(sizeof(WarpStage));
-constexpr long long kWaitLimit = 1ll << 22;
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-    for (long long i = 0; i < kWaitLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
+// A row longer than kChunkNnz is a chunk of its own, streamed by the warp.
+// Reducing epilogues keep per-thread accumulators; Epi::finish combines them
+// per block in a fixed order.
 
 struct Empty {};
 
@@ -277,131 +227,90 @@ struct RowPre<Epi, true> {
     }
 };
 
-struct Chunk {
-    int r0, r1, p0, p1, a0v, a1v, a0i, a1i;
-    __device__ __forceinline__ bool streamed() const { return p1 - p0 > kChunkNnz; }
-};
-
-__device__ __forceinline__ Chunk chunk_at(const TileCsr& A, int t) {
-    const int2 b0 = __ldg(A.tile + t), b1 = __ldg(A.tile + t + 1);
-    Chunk c;
-    c.r0 = b0.x;
-    c.r1 = b1.x;
-    c.p0 = b0.y;
-    c.p1 = b1.y;
-    c.a0v = c.p0 & ~1;
-    c.a1v = max(c.a0v, c.p1 & ~1);
-    c.a0i = c.p0 & ~3;
-    c.a1i = max(c.a0i, c.p1 & ~3);
-    return c;
-}
-
-// Lane 0: both bulk copies of a staged chunk into buffer b of the warp's slice.
-__device__ __forceinline__ void issue_chunk(const TileCsr& A, const Chunk& c, WarpStage& ws, int b) {
-    const unsigned vb = static_cast<unsigned>(c.a1v - c.a0v) * 8u;
-    const unsigned ib = static_cast<unsigned>(c.a1i - c.a0i) * 4u;
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_arrive_expect(&ws.bar[b], vb + ib);
-    if (vb) bulk_load(ws.val[b], A.val + c.a0v, vb, &ws.bar[b]);
-    if (ib) bulk_load(ws.idx[b], A.idx + c.a0i, ib, &ws.bar[b]);
+// Bulk L2 prefetch of [first, last) elements of a 16-byte-aligned array; the
+// range is shrunk to its 16-byte-aligned interior so it never leaves the array.
+template <class T>
+__device__ __forceinline__ void prefetch_l2(const T* base, int first, int last) {
+    constexpr int per = 16 / static_cast<int>(sizeof(T));
+    const int a = (first + per - 1) / per * per, b = last / per * per;
+    if (b > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + a),
+                     "r"(static_cast<unsigned>((b - a) * static_cast<int>(sizeof(T))))
+                     : "memory");
 }
 
 template <class Epi>
-__global__ void __launch_bounds__(kThreads, 4) k_tiled(TileCsr A, const double* __restrict__ v, Epi epi) {
+__global__ void __launch_bounds__(kThreads) k_tiled(TileCsr A, const double* __restrict__ v, Epi epi) {
     using P = RowPre<Epi>;
-    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ double prod[kWarps][kChunkNnz];
     __shared__ double red[kWarps * 8];
     typename Epi::Acc acc;
     acc.init();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpStage& ws = reinterpret_cast<WarpStage*>(dyn)[warp];
     const int nw = gridDim.x * kWarps;
+    double* sp = prod[warp];
     const unsigned full = 0xffffffffu;
-    if (lane == 0) {
-        mbar_init(&ws.bar[0], 1);
-        mbar_init(&ws.bar[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncwarp();
-    unsigned phase = 0;   // bit b: parity to wait for on buffer b
-    unsigned pending = 0; // bit b: a copy into buffer b is in flight
-    bool aborted = false;
     int t = blockIdx.x * kWarps + warp;
-    Chunk cur{};
-    if (t < A.ntiles) {
-        cur = chunk_at(A, t);
-        if (!cur.streamed()) {
-            if (lane == 0) issue_chunk(A, cur, ws, 0);
-            pending |= 1u;
-        }
-    }
-    for (int k = 0; t < A.ntiles; ++k, t += nw) {
-        const int b = k & 1;
+    int2 b0 = t < A.ntiles ? __ldg(A.tile + t) : make_int2(0, 0);
+    int2 b1 = t < A.ntiles ? __ldg(A.tile + t + 1) : make_int2(0, 0);
+    for (; t < A.ntiles; t += nw) {
+        const int r0 = b0.x, r1 = b1.x, p0 = b0.y, p1 = b1.y;
         const int tn = t + nw;
-        Chunk nxt{};
+        int2 n0 = b1, n1 = b1;
         if (tn < A.ntiles) {
-            nxt = chunk_at(A, tn);
-            if (!nxt.streamed()) {
-                if (lane == 0) issue_chunk(A, nxt, ws, b ^ 1);
-                pending |= 2u >> b;  // bit (b ^ 1)
+            n0 = __ldg(A.tile + tn);
+            n1 = __ldg(A.tile + tn + 1);
+            if (lane == 0 && n1.y - n0.y <= kChunkNnz) {
+                prefetch_l2(A.val, n0.y, n1.y);
+                prefetch_l2(A.idx, n0.y, n1.y);
             }
         }
-        const int my = cur.r0 + lane;
-        const bool owns = my < cur.r1;
+        const int my = r0 + lane;
+        const bool owns = my < r1;
         typename P::type pre{};
         int q0 = 0, q1 = 0;
         if (owns) {
             pre = P::load(epi, my);
-            q0 = __ldg(A.ptr + my) - cur.a0v;
-            q1 = __ldg(A.ptr + my + 1) - cur.a0v;
+            q0 = __ldg(A.ptr + my) - p0;
+            q1 = __ldg(A.ptr + my + 1) - p0;
         }
-        if (cur.streamed()) {
+        if (p1 - p0 > kChunkNnz) {
             double s0 = 0.0, s1 = 0.0;
-            int p = cur.p0 + lane;
-            for (; p + 32 < cur.p1; p += 64) {
+            int p = p0 + lane;
+            for (; p + 32 < p1; p += 64) {
                 s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
                 s1 += __ldcs(A.val + p + 32) * __ldg(v + __ldcs(A.idx + p + 32));
             }
-            if (p < cur.p1) s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
+            if (p < p1) s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
             const double s = warp_sum(s0 + s1);
-            if (lane == 0) P::apply(epi, cur.r0, s, pre, acc);
-            cur = nxt;
+            if (lane == 0) P::apply(epi, r0, s, pre, acc);
+            b0 = n0;
+            b1 = n1;
             continue;
         }
-        const bool ok = mbar_wait(&ws.bar[b], (phase >> b) & 1u);
-        phase ^= 1u << b;
-        pending &= ~(1u << b);
-        if (!__all_sync(full, ok)) {
-            if (lane == 0 && A.err) atomicAdd(A.err, 1u);
-            aborted = true;
-            break;
-        }
-        double* sval = ws.val[b];
-        const int* sidx = ws.idx[b];
         int col[kPerLane];
-        double g[kPerLane];
+        double a[kPerLane];
 #pragma unroll
-        for (int e = 0; e < kPerLane; ++e) {
-            const int p = cur.p0 + 32 * e + lane;
-            col[e] = 0;
-            if (p < cur.p1) col[e] = p < cur.a1i ? sidx[p - cur.a0i] : __ldg(A.idx + p);
-        }
-#pragma unroll
-        for (int e = 0; e < kPerLane; ++e)
-            g[e] = cur.p0 + 32 * e + lane < cur.p1 ? __ldg(v + col[e]) : 0.0;
-#pragma unroll
-        for (int e = 0; e < kPerLane; ++e) {
-            const int p = cur.p0 + 32 * e + lane;
-            if (p < cur.p1) {
-                const double a = p < cur.a1v ? sval[p - cur.a0v] : __ldg(A.val + p);
-                sval[p - cur.a0v] = dmul(a, g[e]);
+        for (int k = 0; k < kPerLane; ++k) {
+            const int p = p0 + 32 * k + lane;
+            col[k] = 0;
+            a[k] = 0.0;
+            if (p < p1) {
+                col[k] = __ldcs(A.idx + p);
+                a[k] = __ldcs(A.val + p);
             }
         }
+#pragma unroll
+        for (int k = 0; k < kPerLane; ++k)
+            if (p0 + 32 * k + lane < p1) a[k] = dmul(a[k], __ldg(v + col[k]));
+#pragma unroll
+        for (int k = 0; k < kPerLane; ++k)
+            if (p0 + 32 * k + lane < p1) sp[32 * k + lane] = a[k];
         __syncwarp();
         const int len = q1 - q0;
         if (owns && len <= kShortRow) {
             double s = 0.0;
-            for (int q = q0; q < q1; ++q) s = dadd(s, sval[q]);
+            for (int q = q0; q < q1; ++q) s = dadd(s, sp[q]);
             P::apply(epi, my, s, pre, acc);
         }
         unsigned long_rows = __ballot_sync(full, owns && len > kShortRow);
@@ -410,17 +319,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_tiled(TileCsr A, const double* 
             long_rows &= long_rows - 1;
             const int lq0 = __shfl_sync(full, q0, l), lq1 = __shfl_sync(full, q1, l);
             double s = 0.0;
-            for (int q = lq0 + lane; q < lq1; q += 32) s += sval[q];
+            for (int q = lq0 + lane; q < lq1; q += 32) s += sp[q];
             s = warp_sum(s);
             if (lane == l) P::apply(epi, my, s, pre, acc);
         }
         __syncwarp();
-        cur = nxt;
-    }
-    if (aborted && lane == 0) {
-        // drain copies still in flight before the slice is released
-        for (int b = 0; b < 2; ++b)
-            if (pending & (1u << b)) mbar_wait(&ws.bar[b], (phase >> b) & 1u);
+        b0 = n0;
+        b1 = n1;
     }
     epi.finish(acc, red);
 }
@@ -436,14 +341,14 @@ struct StoreEpi {
 template <class Epi>
 inline int tiled_grid(const TileCsr& A) {
     const void* k = reinterpret_cast<const void*>(&k_tiled<Epi>);
-    return grid_for(k, (A.ntiles + kWarps - 1) / kWarps, kTiledSmem);
+    return grid_for(k, (A.ntiles + kWarps - 1) / kWarps, 0);
 }
 
 template <class Epi>
 inline int launch_tiled(const TileCsr& A, const double* v, const Epi& epi, cudaStream_t stream,
                         int grid) {
     if (A.ntiles == 0) return 0;
-    k_tiled<Epi><<<grid, kThreads, kTiledSmem, stream>>>(A, v, epi);
+    k_tiled<Epi><<<grid, kThreads, 0, stream>>>(A, v, epi);
     return 0;
 }
 
