@@ -182,6 +182,25 @@ def cpu_baseline(inst, target_seconds=12.0):
                       f"c/src without OpenMP) on the same instance, {secs:.2f} s of loop time"}
 
 
+def time_to_kkt(E, A, inst, eps=1e-6, limit_s=90.0):
+    """Wall time of sankhya_b200_pdlp_solve to eps relative KKT on the same instance:
+    plain FP64 PDLP versus FP32 inner iterations with FP64 refinement (and an FP64
+    finish from the refined point). Host arrays in and out, scaling included."""
+    out = {"eps": eps, "relative_kkt": "max(primal, dual, gap) as in GpuPdlp"}
+    for name, prec in (("fp64", E.FP64), ("fp32_refined", E.FP32_REFINE)):
+        s = E.pdlp_default_settings()
+        s.eps_optimal, s.precision, s.time_limit, s.max_iterations = eps, prec, limit_s, 2_000_000
+        t0 = time.perf_counter()
+        rc, x, y, r = E.pdlp_solve(A, inst, s)
+        wall = time.perf_counter() - t0
+        out[name] = {"seconds": round(wall, 3), "status": r["status"], "iterations": r["iterations"],
+                     "refinements": r["refinements"], "objective": float(np.dot(inst["c"], x)),
+                     "kkt": [r["relative_primal_residual"], r["relative_dual_residual"], r["relative_gap"]]}
+    if out["fp64"]["status"] == 0 and out["fp32_refined"]["status"] == 0:
+        out["speedup_mixed_vs_fp64"] = round(out["fp64"]["seconds"] / out["fp32_refined"]["seconds"], 3)
+    return out
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
@@ -294,6 +313,8 @@ def run_engine(args, world, rank, local):
             "e2e": {"value": round(e2e, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": 8 * (4 * n + 3 * m), "d2h_bytes_per_step": 8 * n},
             "gpu_launches": launches, "clocks": clk.summary(), "setup_s": {"generate": round(gen_s, 1)}}
+    if world == 1 and not args.no_time_to_kkt:
+        line["time_to_kkt"] = time_to_kkt(E, A, inst)
     if world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(inst)
@@ -312,6 +333,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-time-to-kkt", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
     try:

@@ -176,6 +176,47 @@ SANKHYA_CUDA_API int sankhya_b200_pdlp_solve(
     const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
     double* x_out, double* y_out, SankhyaB200PdlpResult* result);
 
+/* ------------------------------------------------------- batched LPs */
+
+typedef struct SankhyaB200BatchSettings {
+    int struct_version;  /* 1 */
+    int max_iterations;  /* per LP (100000, sk_solve's default)              */
+    int check_every;     /* 20, as in sk_solve                               */
+    int reserved;
+    double primal_tol;   /* 1e-7 */
+    double dual_tol;     /* 1e-7 */
+    double time_limit;   /* seconds for the whole batch, <= 0 for none        */
+} SankhyaB200BatchSettings;
+
+typedef struct SankhyaB200BatchResult {
+    int status;          /* 0 gates passed, 1 iteration limit, 2 time limit    */
+    int iterations;      /* iterations this LP ran before it was frozen        */
+    double objective;    /* c'x over the LP's columns                          */
+    double row_violation;/* values of the LP's last checkpoint                 */
+    double step;
+    double dual_step;
+    double anorm;
+} SankhyaB200BatchResult;
+
+SANKHYA_CUDA_API void sankhya_b200_batch_default_settings(SankhyaB200BatchSettings* settings);
+
+/* Many independent LPs in one set of launches. No counterpart in the reference:
+   it solves LPs one at a time (the node relaxations of c/src/sk_milp.c:431-459
+   each call the simplex). The LPs are given as one block-diagonal device matrix:
+   LP k owns rows [row_segments[k], row_segments[k+1]) and columns
+   [col_segments[k], col_segments[k+1]); a nonzero outside its LP's block is
+   rejected. Each LP runs the first-order loop of sk_solve (c/src/sk_solve.c:849-954:
+   diagonal steps from its own row/column masses, its own 20-iteration gates and
+   its own anorm) and is frozen as soon as its gates pass, so its iterates equal a
+   separate solve's. Host arrays are concatenated per LP; bounds use the 1e30
+   sentinel. Returns 0 or -1. */
+SANKHYA_CUDA_API int sankhya_b200_batch_pdhg(
+    const SankhyaCudaCSR* block_matrix, int batch, const int* row_segments, const int* col_segments,
+    const double* c, const double* row_lower, const double* row_upper,
+    const double* col_lower, const double* col_upper,
+    const SankhyaB200BatchSettings* settings, double* x_out, double* y_out,
+    SankhyaB200BatchResult* results);
+
 /* Equilibration factors computed on the device, without solving: row_scale
    (rows) and col_scale (cols) such that the scaled matrix is
    diag(row_scale) A diag(col_scale). scaling is a SANKHYA_B200_SCALE_* mask:

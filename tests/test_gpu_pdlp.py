@@ -94,3 +94,41 @@ def test_warm_start_from_solution(engine, instances):
     rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-8))
     rc2, x2, y2, r2 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-6), x0=x, y0=y)
     assert rc2 == 0 and r2["status"] == 0 and r2["iterations"] <= 256, r2
+
+
+# ------------------------------------------------------------------ FP32 refinement
+
+@pytest.mark.parametrize("case", range(len(HAND)))
+def test_fp32_refined_hand_lps(engine, instances, case):
+    spec, ok = HAND[case]
+    inst = instances.small_dense_lp(**spec)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, precision=engine.FP32_REFINE))
+    assert rc == 0 and r["status"] == 0, r
+    assert r["refinements"] >= 1
+    assert ok(x), (x, r)
+
+
+@pytest.mark.parametrize("name,seed,m,n,per_col", [("lp60", 12, 60, 150, 4), ("lp300", 11, 300, 700, 5)])
+def test_fp32_refined_reaches_simplex_objective(engine, instances, golden_dir, name, seed, m, n, per_col):
+    """FP32 inner iterations, FP64 refinement: the FP64 certificate reaches 1e-8 and the
+    objective matches the reference simplex to 1e-6 relative."""
+    ref = json.load(open(os.path.join(golden_dir, f"simplex_{name}.json")))
+    inst = instances.lp_uniform(seed, m, n, per_col)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, precision=engine.FP32_REFINE, eps_optimal=1e-8))
+    assert rc == 0 and r["status"] == 0, r
+    assert max(r["relative_primal_residual"], r["relative_dual_residual"], r["relative_gap"]) <= 1e-8
+    obj = float(np.dot(inst["c"], x))
+    assert abs(obj - ref["objective"]) <= 1e-6 * (1 + abs(ref["objective"])), (obj, ref)
+
+
+def test_fp32_refined_agrees_with_fp64_on_power_law(engine, instances):
+    inst = instances.lp_powerlaw(21, 4000, 8000, 80000)
+    A = engine.Matrix.from_instance(inst)
+    rc64, x64, y64, r64 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-5, time_limit=60.0))
+    rc32, x32, y32, r32 = engine.pdlp_solve(A, inst, settings(engine, precision=engine.FP32_REFINE, eps_optimal=1e-5,
+                                                              time_limit=60.0))
+    assert rc64 == 0 and rc32 == 0 and r64["status"] == 0 and r32["status"] == 0, (r64, r32)
+    o64, o32 = float(np.dot(inst["c"], x64)), float(np.dot(inst["c"], x32))
+    assert abs(o64 - o32) <= 1e-4 * (1 + abs(o64))

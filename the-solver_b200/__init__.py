@@ -33,6 +33,7 @@ REFERENCE_SYMBOLS = (
 EXTENSION_SYMBOLS = (
     "sankhya_b200_set_timing", "sankhya_b200_last_timing", "sankhya_b200_pdhg_loop",
     "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve", "sankhya_b200_scale_factors",
+    "sankhya_b200_batch_default_settings", "sankhya_b200_batch_pdhg",
 )
 
 _lib = None
@@ -125,6 +126,20 @@ class PdlpResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchSettings(C.Structure):
+    """SankhyaB200BatchSettings."""
+    _fields_ = [("struct_version", C.c_int), ("max_iterations", C.c_int), ("check_every", C.c_int),
+                ("reserved", C.c_int), ("primal_tol", C.c_double), ("dual_tol", C.c_double),
+                ("time_limit", C.c_double)]
+
+
+class BatchResult(C.Structure):
+    """SankhyaB200BatchResult."""
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("objective", C.c_double),
+                ("row_violation", C.c_double), ("step", C.c_double), ("dual_step", C.c_double),
+                ("anorm", C.c_double)]
+
+
 SCALE_RUIZ, SCALE_POCK_CHAMBOLLE, SCALE_POW2 = 1, 2, 4
 FP64, FP32_REFINE = 0, 1
 
@@ -161,6 +176,11 @@ def _declare(L):
         L.sankhya_b200_pdlp_solve.argtypes = [P(CSR), dptr, dptr, dptr, dptr, dptr, P(PdlpSettings), dptr,
                                               dptr, dptr, dptr, P(PdlpResult)]
         L.sankhya_b200_scale_factors.argtypes = [P(CSR), C.c_int, C.c_int, C.c_double, dptr, dptr]
+    if hasattr(L, "sankhya_b200_batch_pdhg"):
+        L.sankhya_b200_batch_default_settings.argtypes = [P(BatchSettings)]
+        L.sankhya_b200_batch_default_settings.restype = None
+        L.sankhya_b200_batch_pdhg.argtypes = [P(CSR), C.c_int, iptr, iptr, dptr, dptr, dptr, dptr, dptr,
+                                              P(BatchSettings), dptr, dptr, P(BatchResult)]
 
 
 def _d(a):
@@ -307,3 +327,44 @@ def scale_factors(matrix: Matrix, scaling: int, ruiz_iterations: int = 100, ruiz
     rc = lib().sankhya_b200_scale_factors(C.byref(matrix.handle), int(scaling), int(ruiz_iterations),
                                           float(ruiz_tolerance), _p(r), _p(c))
     return rc, r, c
+
+
+def block_diagonal(instances_list):
+    """Concatenates LP instance dicts into one block-diagonal instance plus the
+    row / column segment offsets."""
+    ptrs, idxs, vals = [np.zeros(1, dtype=np.int64)], [], []
+    rseg, cseg = [0], [0]
+    nz = 0
+    for inst in instances_list:
+        ptrs.append(inst["ptr"][1:].astype(np.int64) + nz)
+        idxs.append(inst["idx"].astype(np.int64) + cseg[-1])
+        vals.append(inst["val"])
+        nz += int(inst["ptr"][-1])
+        rseg.append(rseg[-1] + inst["m"])
+        cseg.append(cseg[-1] + inst["n"])
+    cat = lambda k: np.concatenate([i[k] for i in instances_list])
+    out = dict(m=rseg[-1], n=cseg[-1], ptr=np.concatenate(ptrs).astype(np.int32),
+               idx=np.concatenate(idxs).astype(np.int32), val=np.concatenate(vals),
+               c=cat("c"), rl=cat("rl"), ru=cat("ru"), cl=cat("cl"), cu=cat("cu"))
+    return out, np.asarray(rseg, dtype=np.int32), np.asarray(cseg, dtype=np.int32)
+
+
+def batch_default_settings() -> BatchSettings:
+    s = BatchSettings()
+    lib().sankhya_b200_batch_default_settings(C.byref(s))
+    return s
+
+
+def batch_pdhg(matrix: Matrix, inst, row_segments, col_segments, s: BatchSettings | None = None, want_dual=False):
+    """Batched sk_solve-style PDHG over a block-diagonal matrix; returns (rc, x, y, results list)."""
+    s = s or batch_default_settings()
+    rseg = np.ascontiguousarray(row_segments, dtype=np.int32)
+    cseg = np.ascontiguousarray(col_segments, dtype=np.int32)
+    k = rseg.shape[0] - 1
+    x = np.zeros(matrix.handle.cols)
+    y = np.zeros(matrix.handle.rows) if want_dual else None
+    res = (BatchResult * k)()
+    rc = lib().sankhya_b200_batch_pdhg(C.byref(matrix.handle), k, rseg.ctypes.data_as(iptr), cseg.ctypes.data_as(iptr),
+                                       _p(_d(inst["c"])), _p(_d(inst["rl"])), _p(_d(inst["ru"])), _p(_d(inst["cl"])),
+                                       _p(_d(inst["cu"])), C.byref(s), _p(x), _p(y), res)
+    return rc, x, y, [{f: getattr(r, f) for f, _ in BatchResult._fields_} for r in res]

@@ -48,14 +48,26 @@ constexpr int kShortRow = 32;          // rows up to this length: owning lane, s
 // the chunk boundaries as (row, first nonzero) pairs, ntiles + 1 of them.
 std::vector<int> build_tiles(int rows, const int* row_offsets);
 
-struct TileCsr {
+// A CSR with its warp-chunk schedule; T is the value type (double, or float
+// for the FP32 inner iterations of the refined PDLP).
+template <class T>
+struct TileCsrT {
     int rows = 0, cols = 0, nnz = 0, ntiles = 0;
     const int* ptr = nullptr;
     const int* idx = nullptr;
-    const double* val = nullptr;
+    const T* val = nullptr;
     const int2* tile = nullptr;   // chunk boundaries: (first row, first nonzero)
     unsigned int* err = nullptr;  // counts bounded device waits that gave up (may be null)
+
+    template <class U>
+    TileCsrT<U> with_values(const U* v) const {
+        TileCsrT<U> o;
+        o.rows = rows; o.cols = cols; o.nnz = nnz; o.ntiles = ntiles;
+        o.ptr = ptr; o.idx = idx; o.val = v; o.tile = tile; o.err = err;
+        return o;
+    }
 };
+using TileCsr = TileCsrT<double>;
 
 // Owns everything a solve needs for one matrix beyond the caller's CSR.
 struct Plan {
@@ -106,6 +118,8 @@ __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float dadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float dmul(float a, float b) { return __fmul_rn(a, b); }
 
 // cuda/src/sankhya_cuda_lp.cu:13-17: only IEEE infinities are absent bounds.
 __device__ __forceinline__ double box_ieee(double v, double lo, double hi) {
@@ -169,7 +183,8 @@ __device__ void block_store(Slots<NS, SumMask>& acc, double* __restrict__ partia
     __syncthreads();
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     return v;
@@ -212,8 +227,8 @@ template <class Epi, bool = HasLoad<Epi>::value>
 struct RowPre {
     using type = Empty;
     static __device__ __forceinline__ type load(const Epi&, int) { return {}; }
-    static __device__ __forceinline__ void apply(const Epi& e, int r, double s, const type&,
-                                                 typename Epi::Acc& acc) {
+    template <class T>
+    static __device__ __forceinline__ void apply(const Epi& e, int r, T s, const type&, typename Epi::Acc& acc) {
         e.row(r, s, acc);
     }
 };
@@ -221,8 +236,8 @@ template <class Epi>
 struct RowPre<Epi, true> {
     using type = typename Epi::Row;
     static __device__ __forceinline__ type load(const Epi& e, int r) { return e.load(r); }
-    static __device__ __forceinline__ void apply(const Epi& e, int r, double s, const type& pre,
-                                                 typename Epi::Acc& acc) {
+    template <class T>
+    static __device__ __forceinline__ void apply(const Epi& e, int r, T s, const type& pre, typename Epi::Acc& acc) {
         e.store(r, s, pre, acc);
     }
 };
@@ -239,16 +254,16 @@ __device__ __forceinline__ void prefetch_l2(const T* base, int first, int last) 
                      : "memory");
 }
 
-template <class Epi>
-__global__ void __launch_bounds__(kThreads) k_tiled(TileCsr A, const double* __restrict__ v, Epi epi) {
+template <class Epi, class T>
+__global__ void __launch_bounds__(kThreads) k_tiled(TileCsrT<T> A, const T* __restrict__ v, Epi epi) {
     using P = RowPre<Epi>;
-    __shared__ double prod[kWarps][kChunkNnz];
+    __shared__ T prod[kWarps][kChunkNnz];
     __shared__ double red[kWarps * 8];
     typename Epi::Acc acc;
     acc.init();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nw = gridDim.x * kWarps;
-    double* sp = prod[warp];
+    T* sp = prod[warp];
     const unsigned full = 0xffffffffu;
     int t = blockIdx.x * kWarps + warp;
     int2 b0 = t < A.ntiles ? __ldg(A.tile + t) : make_int2(0, 0);
@@ -275,26 +290,26 @@ __global__ void __launch_bounds__(kThreads) k_tiled(TileCsr A, const double* __r
             q1 = __ldg(A.ptr + my + 1) - p0;
         }
         if (p1 - p0 > kChunkNnz) {
-            double s0 = 0.0, s1 = 0.0;
+            T s0 = T(0), s1 = T(0);
             int p = p0 + lane;
             for (; p + 32 < p1; p += 64) {
                 s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
                 s1 += __ldcs(A.val + p + 32) * __ldg(v + __ldcs(A.idx + p + 32));
             }
             if (p < p1) s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
-            const double s = warp_sum(s0 + s1);
+            const T s = warp_sum(s0 + s1);
             if (lane == 0) P::apply(epi, r0, s, pre, acc);
             b0 = n0;
             b1 = n1;
             continue;
         }
         int col[kPerLane];
-        double a[kPerLane];
+        T a[kPerLane];
 #pragma unroll
         for (int k = 0; k < kPerLane; ++k) {
             const int p = p0 + 32 * k + lane;
             col[k] = 0;
-            a[k] = 0.0;
+            a[k] = T(0);
             if (p < p1) {
                 col[k] = __ldcs(A.idx + p);
                 a[k] = __ldcs(A.val + p);
@@ -309,7 +324,7 @@ __global__ void __launch_bounds__(kThreads) k_tiled(TileCsr A, const double* __r
         __syncwarp();
         const int len = q1 - q0;
         if (owns && len <= kShortRow) {
-            double s = 0.0;
+            T s = T(0);
             for (int q = q0; q < q1; ++q) s = dadd(s, sp[q]);
             P::apply(epi, my, s, pre, acc);
         }
@@ -318,7 +333,7 @@ __global__ void __launch_bounds__(kThreads) k_tiled(TileCsr A, const double* __r
             const int l = __ffs(long_rows) - 1;
             long_rows &= long_rows - 1;
             const int lq0 = __shfl_sync(full, q0, l), lq1 = __shfl_sync(full, q1, l);
-            double s = 0.0;
+            T s = T(0);
             for (int q = lq0 + lane; q < lq1; q += 32) s += sp[q];
             s = warp_sum(s);
             if (lane == l) P::apply(epi, my, s, pre, acc);
@@ -331,24 +346,25 @@ __global__ void __launch_bounds__(kThreads) k_tiled(TileCsr A, const double* __r
 }
 
 // Plain product y = A v.
-struct StoreEpi {
-    double* y;
+template <class T = double>
+struct StoreEpiT {
+    T* y;
     using Acc = NoAcc;
-    __device__ __forceinline__ void row(int r, double s, NoAcc&) const { y[r] = s; }
+    __device__ __forceinline__ void row(int r, T s, NoAcc&) const { y[r] = s; }
     __device__ __forceinline__ void finish(NoAcc&, double*) const {}
 };
+using StoreEpi = StoreEpiT<double>;
 
-template <class Epi>
-inline int tiled_grid(const TileCsr& A) {
-    const void* k = reinterpret_cast<const void*>(&k_tiled<Epi>);
+template <class Epi, class T = double>
+inline int tiled_grid(const TileCsrT<T>& A) {
+    const void* k = reinterpret_cast<const void*>(&k_tiled<Epi, T>);
     return grid_for(k, (A.ntiles + kWarps - 1) / kWarps, 0);
 }
 
-template <class Epi>
-inline int launch_tiled(const TileCsr& A, const double* v, const Epi& epi, cudaStream_t stream,
-                        int grid) {
+template <class Epi, class T>
+inline int launch_tiled(const TileCsrT<T>& A, const T* v, const Epi& epi, cudaStream_t stream, int grid) {
     if (A.ntiles == 0) return 0;
-    k_tiled<Epi><<<grid, kThreads, 0, stream>>>(A, v, epi);
+    k_tiled<Epi, T><<<grid, kThreads, 0, stream>>>(A, v, epi);
     return 0;
 }
 

@@ -1,4 +1,5 @@
-// Restarted adaptive PDLP behind sankhya_b200_pdlp_solve.
+// Restarted adaptive PDLP behind sankhya_b200_pdlp_solve, in FP64 or with
+// FP32 inner iterations inside an FP64 iterative-refinement loop.
 //
 // The algorithm is the reference's GpuPdlp (src/cuda/GpuPdlp.cpp:179-534,
 // src/cuda/PdlpKernels.cu:71-518): power-iteration ||A||_2, eta = 0.9/||A||,
@@ -6,19 +7,28 @@
 // accept/reject decided on the device, restart to the better of current and
 // average at the 0.2 / 0.8 / 0.36 criteria, log-smoothed omega update,
 // relative-KKT termination. Scaling (Ruiz, Pock-Chambolle, power-of-two) is
-// computed and applied on the device.
+// computed and applied on the device in FP64.
 //
 // Per adaptive iteration three launches, all reading eta / omega / the accept
 // flag from device memory so a whole window is one CUDA graph:
 //   K1  elementwise: commit the previous candidate if accepted (x, y, sums,
 //       A x, A x_prev), then y_cand = prox(y + sigma (2 A x - A x_prev))
-//   K2  A'-side tiles: x_cand = proj(x - tau (c + A'y_cand)), block sums of |dx|^2
-//   K3  A-side tiles:  A x_cand, block sums of |dy|^2 and dy.(A dx); the last
+//   K2  A'-side chunks: x_cand = proj(x - tau (c + A'y_cand)), block sums of |dx|^2
+//   K3  A-side chunks:  A x_cand, block sums of |dy|^2 and dy.(A dx); the last
 //       block to finish combines all partials in a fixed order and writes the
 //       new eta and the accept flag (PdlpKernels.cu:405-494).
 // The window ends with a commit, the residual sums of the current and of the
 // average iterate (PdlpKernels.cu:101-209, fused into the two products), and
-// one 200-byte copy to the host, which makes the restart decision.
+// one small copy to the host, which makes the restart decision.
+//
+// FP32_REFINE: the iterations run with FP32 matrix values and vectors (FP32
+// accumulation in the products, FP64 for the restart / KKT reductions) on the
+// scaled problem until the FP64-evaluated relative KKT reaches max(eps, 1e-4);
+// the point, the primal weight and the step size then seed an FP64 finish to
+// eps. (A correction-LP refinement in the manner of Gleixner, Steffy and Wolter
+// was tried first and stalled on boxed LPs: the refined problem's bound terms
+// ap (u - x) multiply the FP32 reduced-cost noise in the dual objective, so its
+// relative gap never reached the inner tolerance.)
 #include "engine.cuh"
 
 #include <algorithm>
@@ -52,23 +62,27 @@ struct PdlpState {
     unsigned int pad;
 };
 
-__device__ __forceinline__ double clampf(double v, double lo, double hi) { return fmin(fmax(v, lo), hi); }
+template <class T>
+__device__ __forceinline__ T clampf(T v, T lo, T hi) {
+    return fmin(fmax(v, lo), hi);
+}
 
 // ------------------------------------------------------------ iteration kernels
 
 // K1 (PdlpKernels.cu:499-518 commit, then :377-389 dual candidate)
-__global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, double* __restrict__ x,
-                              const double* __restrict__ x_cand, double* __restrict__ x_sum, double* __restrict__ y,
-                              double* __restrict__ y_cand, double* __restrict__ y_sum, double* __restrict__ ax,
-                              double* __restrict__ ax_prev, const double* __restrict__ ax_cand,
-                              const double* __restrict__ rl, const double* __restrict__ ru, int make_candidate) {
+template <class T>
+__global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, T* __restrict__ x,
+                              const T* __restrict__ x_cand, T* __restrict__ x_sum, T* __restrict__ y,
+                              T* __restrict__ y_cand, T* __restrict__ y_sum, T* __restrict__ ax, T* __restrict__ ax_prev,
+                              const T* __restrict__ ax_cand, const T* __restrict__ rl, const T* __restrict__ ru,
+                              int make_candidate) {
     const bool acc = st->accepted != 0.0;
-    const double sigma = st->eta * st->omega;
+    const T sigma = static_cast<T>(st->eta * st->omega);
     const int stride = blockDim.x * gridDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-        double yi = y[i], axi = ax[i], axp = ax_prev[i];
+        T yi = y[i], axi = ax[i], axp = ax_prev[i];
         if (acc) {
-            const double yc = y_cand[i];
+            const T yc = y_cand[i];
             yi = yc;
             y[i] = yc;
             y_sum[i] += yc;
@@ -78,13 +92,13 @@ __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, double* 
             ax[i] = axi;
         }
         if (make_candidate) {
-            const double v = yi + sigma * (2.0 * axi - axp);
-            y_cand[i] = v - sigma * clampf(v / sigma, rl[i], ru[i]);
+            const T v = yi + sigma * (T(2) * axi - axp);
+            y_cand[i] = v - sigma * clampf<T>(v / sigma, rl[i], ru[i]);
         }
     }
     if (acc) {
         for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
-            const double xc = x_cand[j];
+            const T xc = x_cand[j];
             x[j] = xc;
             x_sum[j] += xc;
         }
@@ -92,49 +106,51 @@ __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, double* 
 }
 
 // K2 (PdlpKernels.cu:391-400 primal candidate + the |dx|^2 part of :405-430)
+template <class T>
 struct PrimalCandEpi {
     const PdlpState* st;
-    const double* __restrict__ x;
-    const double* __restrict__ c;
-    const double* __restrict__ cl;
-    const double* __restrict__ cu;
-    double* __restrict__ x_cand;
+    const T* __restrict__ x;
+    const T* __restrict__ c;
+    const T* __restrict__ cl;
+    const T* __restrict__ cu;
+    T* __restrict__ x_cand;
     double* __restrict__ partial;
     using Acc = Slots<1, 1u>;
     struct Row {
-        double x, c, lo, hi;
+        T x, c, lo, hi;
     };
     __device__ __forceinline__ Row load(int j) const { return Row{x[j], c[j], cl[j], cu[j]}; }
-    __device__ __forceinline__ void store(int j, double aty, const Row& r, Acc& acc) const {
-        const double tau = st->eta / st->omega;
-        const double xc = clampf(r.x - tau * (r.c + aty), r.lo, r.hi);
+    __device__ __forceinline__ void store(int j, T aty, const Row& r, Acc& acc) const {
+        const T tau = static_cast<T>(st->eta / st->omega);
+        const T xc = clampf<T>(r.x - tau * (r.c + aty), r.lo, r.hi);
         x_cand[j] = xc;
-        const double dx = xc - r.x;
+        const double dx = static_cast<double>(xc) - static_cast<double>(r.x);
         acc.add(0, dx * dx);
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
 };
 
 // K3 (A x_cand, |dy|^2, dy.(A x_cand - A x), then PdlpKernels.cu:460-494 in the last block)
+template <class T>
 struct ProbeEpi {
     PdlpState* st;
-    const double* __restrict__ y;
-    const double* __restrict__ y_cand;
-    const double* __restrict__ ax;
-    double* __restrict__ ax_cand;
-    double* __restrict__ partial;        // this kernel's [gridDim.x * 2]
+    const T* __restrict__ y;
+    const T* __restrict__ y_cand;
+    const T* __restrict__ ax;
+    T* __restrict__ ax_cand;
+    double* __restrict__ partial;           // this kernel's [gridDim.x * 2]
     const double* __restrict__ partial_dx;  // K2's [grid_dx]
     int grid_dx;
     using Acc = Slots<2, 3u>;
     struct Row {
-        double y, yc, ax;
+        T y, yc, ax;
     };
     __device__ __forceinline__ Row load(int i) const { return Row{y[i], y_cand[i], ax[i]}; }
-    __device__ __forceinline__ void store(int i, double axc, const Row& r, Acc& acc) const {
+    __device__ __forceinline__ void store(int i, T axc, const Row& r, Acc& acc) const {
         ax_cand[i] = axc;
-        const double dy = r.yc - r.y;
+        const double dy = static_cast<double>(r.yc) - static_cast<double>(r.y);
         acc.add(0, dy * dy);
-        acc.add(1, dy * (axc - r.ax));
+        acc.add(1, dy * (static_cast<double>(axc) - static_cast<double>(r.ax)));
     }
     __device__ void finish(Acc& acc, double* smem) const {
         block_store(acc, partial, smem);
@@ -193,36 +209,37 @@ struct ProbeEpi {
 };
 
 // Fixed-step path (PdlpKernels.cu:71-97): dual on A x_bar, primal on A'y, with sums.
+template <class T>
 struct DualFixedEpi {
-    const PdlpState* st;
-    double* __restrict__ y;
-    double* __restrict__ y_sum;
-    const double* __restrict__ rl;
-    const double* __restrict__ ru;
-    double sigma;
+    T* __restrict__ y;
+    T* __restrict__ y_sum;
+    const T* __restrict__ rl;
+    const T* __restrict__ ru;
+    T sigma;
     using Acc = NoAcc;
-    __device__ __forceinline__ void row(int i, double axb, Acc&) const {
-        const double v = y[i] + sigma * axb;
-        const double yi = v - sigma * clampf(v / sigma, rl[i], ru[i]);
+    __device__ __forceinline__ void row(int i, T axb, Acc&) const {
+        const T v = y[i] + sigma * axb;
+        const T yi = v - sigma * clampf<T>(v / sigma, rl[i], ru[i]);
         y[i] = yi;
         y_sum[i] += yi;
     }
     __device__ __forceinline__ void finish(Acc&, double*) const {}
 };
 
+template <class T>
 struct PrimalFixedEpi {
-    double* __restrict__ x;
-    double* __restrict__ x_bar;
-    double* __restrict__ x_sum;
-    const double* __restrict__ c;
-    const double* __restrict__ cl;
-    const double* __restrict__ cu;
-    double tau;
+    T* __restrict__ x;
+    T* __restrict__ x_bar;
+    T* __restrict__ x_sum;
+    const T* __restrict__ c;
+    const T* __restrict__ cl;
+    const T* __restrict__ cu;
+    T tau;
     using Acc = NoAcc;
-    __device__ __forceinline__ void row(int j, double aty, Acc&) const {
-        const double xj = x[j];
-        const double xn = clampf(xj - tau * (c[j] + aty), cl[j], cu[j]);
-        x_bar[j] = 2.0 * xn - xj;
+    __device__ __forceinline__ void row(int j, T aty, Acc&) const {
+        const T xj = x[j];
+        const T xn = clampf<T>(xj - tau * (c[j] + aty), cl[j], cu[j]);
+        x_bar[j] = T(2) * xn - xj;
         x[j] = xn;
         x_sum[j] += xn;
     }
@@ -230,48 +247,56 @@ struct PrimalFixedEpi {
 };
 
 // ----------------------------------------------------------- residual kernels
-// PdlpKernels.cu:101-209 split over the two products. Row slots (sums):
-// 0 |Ax - proj(Ax)|^2, 1 |y|^2, 2 |y - y_restart|^2, 3 -support(y).
+// PdlpKernels.cu:101-209 split over the two products, accumulated in FP64.
+// Row slots: 0 |Ax - proj(Ax)|^2, 1 |y|^2, 2 |y - y_restart|^2, 3 -support(y)
+// (sums), 4 max |Ax - proj(Ax)| (max).
+template <class T>
 struct ResRowsEpi {
-    const double* __restrict__ y;
-    const double* __restrict__ y_restart;
-    const double* __restrict__ rl;
-    const double* __restrict__ ru;
-    double* __restrict__ ax_out;  // may be null
+    const T* __restrict__ y;
+    const T* __restrict__ y_restart;
+    const T* __restrict__ rl;
+    const T* __restrict__ ru;
+    T* __restrict__ ax_out;  // may be null
     double* __restrict__ partial;
-    using Acc = Slots<4, 0xFu>;
-    __device__ __forceinline__ void row(int i, double axi, Acc& acc) const {
-        if (ax_out) ax_out[i] = axi;
-        const double lo = rl[i], hi = ru[i], yi = y[i];
-        const double pr = axi - clampf(axi, lo, hi);
+    using Acc = Slots<5, 0xFu>;
+    __device__ __forceinline__ void row(int i, T axt, Acc& acc) const {
+        if (ax_out) ax_out[i] = axt;
+        const double axi = axt, lo = rl[i], hi = ru[i], yi = y[i];
+        const double pr = axi - fmin(fmax(axi, lo), hi);
         acc.add(0, pr * pr);
         acc.add(1, yi * yi);
-        const double dy = yi - y_restart[i];
+        const double dy = yi - static_cast<double>(y_restart[i]);
         acc.add(2, dy * dy);
         double support = 0.0;
         if (yi > 0.0) support = isfinite(hi) ? yi * hi : 0.0;
         else if (yi < 0.0) support = isfinite(lo) ? yi * lo : 0.0;
         acc.add(3, -support);
+        acc.max(4, fabs(pr));
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
 };
 
-// Column slots (sums): 0 dual violation^2, 1 dual objective column terms,
-// 2 c'x, 3 |x|^2, 4 |x - x_restart|^2.
+// Column slots: 0 dual violation^2, 1 dual objective column terms, 2 c'x,
+// 3 |x|^2, 4 |x - x_restart|^2 (sums), 5 max |x - proj(x - (c + A'y))| (max;
+// the column KKT residual, which sees reduced costs of interior variables even
+// when every bound is finite and the dual violation itself is zero).
+template <class T>
 struct ResColsEpi {
-    const double* __restrict__ x;
-    const double* __restrict__ x_restart;
-    const double* __restrict__ c;
-    const double* __restrict__ cl;
-    const double* __restrict__ cu;
+    const T* __restrict__ x;
+    const T* __restrict__ x_restart;
+    const T* __restrict__ c;
+    const T* __restrict__ cl;
+    const T* __restrict__ cu;
+    T* __restrict__ aty_out;  // may be null
     double* __restrict__ partial;
-    using Acc = Slots<5, 0x1Fu>;
-    __device__ __forceinline__ void row(int j, double aty, Acc& acc) const {
-        const double xj = x[j], lo = cl[j], hi = cu[j];
-        const double r = c[j] + aty;
-        acc.add(2, c[j] * xj);
+    using Acc = Slots<6, 0x1Fu>;
+    __device__ __forceinline__ void row(int j, T atyt, Acc& acc) const {
+        if (aty_out) aty_out[j] = atyt;
+        const double xj = x[j], lo = cl[j], hi = cu[j], cj = c[j];
+        const double r = cj + static_cast<double>(atyt);
+        acc.add(2, cj * xj);
         acc.add(3, xj * xj);
-        const double dx = xj - x_restart[j];
+        const double dx = xj - static_cast<double>(x_restart[j]);
         acc.add(4, dx * dx);
         const bool lf = isfinite(lo), hf = isfinite(hi);
         double viol = 0.0, term = 0.0;
@@ -288,78 +313,90 @@ struct ResColsEpi {
         }
         acc.add(0, viol * viol);
         acc.add(1, term);
+        acc.max(5, fabs(xj - fmin(fmax(xj - r, lo), hi)));
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
 };
 
-// out[0..7] in the reference's PdlpResiduals order (PdlpKernels.cuh), plus a
-// copy of the step state; clears the accept flag after the window commit.
+// out[0..7] in the reference's PdlpResiduals order (PdlpKernels.cuh), then the
+// step state, then out[12] max primal residual, out[13] max column KKT residual;
+// clears the accept flag after the window commit.
 __global__ void k_res_combine(const double* __restrict__ prow, int nrow_blocks, const double* __restrict__ pcol,
                               int ncol_blocks, double* __restrict__ out, PdlpState* st, int clear_accept) {
-    __shared__ double red[9][kThreads];
-    double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int g = threadIdx.x; g < nrow_blocks; g += kThreads)
-        for (int k = 0; k < 4; ++k) v[k] += prow[g * 4 + k];
-    for (int g = threadIdx.x; g < ncol_blocks; g += kThreads)
-        for (int k = 0; k < 5; ++k) v[4 + k] += pcol[g * 5 + k];
-    for (int k = 0; k < 9; ++k) red[k][threadIdx.x] = v[k];
+    __shared__ double red[11][kThreads];
+    double v[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int g = threadIdx.x; g < nrow_blocks; g += kThreads) {
+        for (int k = 0; k < 4; ++k) v[k] += prow[g * 5 + k];
+        v[4] = fmax(v[4], prow[g * 5 + 4]);
+    }
+    for (int g = threadIdx.x; g < ncol_blocks; g += kThreads) {
+        for (int k = 0; k < 5; ++k) v[5 + k] += pcol[g * 6 + k];
+        v[10] = fmax(v[10], pcol[g * 6 + 5]);
+    }
+    for (int k = 0; k < 11; ++k) red[k][threadIdx.x] = v[k];
     __syncthreads();
     for (int s = kThreads / 2; s > 0; s >>= 1) {
         if (threadIdx.x < s)
-            for (int k = 0; k < 9; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+            for (int k = 0; k < 11; ++k)
+                red[k][threadIdx.x] = (k == 4 || k == 10) ? fmax(red[k][threadIdx.x], red[k][threadIdx.x + s])
+                                                          : red[k][threadIdx.x] + red[k][threadIdx.x + s];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         // primal_residual_sq, dual_residual_sq, primal_objective, dual_objective,
         // x_norm_sq, y_norm_sq, primal_move_sq, dual_move_sq
         out[0] = red[0][0];
-        out[1] = red[4][0];
-        out[2] = red[6][0];
-        out[3] = red[5][0] + red[3][0];
-        out[4] = red[7][0];
+        out[1] = red[5][0];
+        out[2] = red[7][0];
+        out[3] = red[6][0] + red[3][0];
+        out[4] = red[8][0];
         out[5] = red[1][0];
-        out[6] = red[8][0];
+        out[6] = red[9][0];
         out[7] = red[2][0];
         out[8] = st->eta;
         out[9] = st->accept_count;
         out[10] = st->updates;
         out[11] = st->omega;
+        out[12] = red[4][0];
+        out[13] = red[10][0];
         if (clear_accept) st->accepted = 0.0;
     }
 }
 
 // x_avg = (1/terms) x_sum (GpuPdlp.cpp:371-390 with the divisor on the device)
-__global__ void k_average(int n, int m, const PdlpState* __restrict__ st, int adaptive, const double* __restrict__ x_sum,
-                          const double* __restrict__ y_sum, double* __restrict__ x_avg, double* __restrict__ y_avg) {
+template <class T>
+__global__ void k_average(int n, int m, const PdlpState* __restrict__ st, int adaptive, const T* __restrict__ x_sum,
+                          const T* __restrict__ y_sum, T* __restrict__ x_avg, T* __restrict__ y_avg) {
     double terms = adaptive ? st->accept_count - st->accepted_at_restart : st->terms_fixed;
     if (terms < 1.0) terms = 1.0;
-    const double scale = 1.0 / terms;
+    const T scale = static_cast<T>(1.0 / terms);
     const int stride = blockDim.x * gridDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) x_avg[j] = scale * x_sum[j];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y_avg[i] = scale * y_sum[i];
 }
 
 // Restart (GpuPdlp.cpp:453-497) as one elementwise pass.
-__global__ void k_restart(int n, int m, int to_average, int adaptive, double* __restrict__ x, double* __restrict__ y,
-                          double* __restrict__ x_bar, const double* __restrict__ x_avg,
-                          const double* __restrict__ y_avg, double* __restrict__ ax, double* __restrict__ ax_prev,
-                          const double* __restrict__ ax_avg, double* __restrict__ x_sum, double* __restrict__ y_sum,
-                          double* __restrict__ x_restart, double* __restrict__ y_restart, PdlpState* st) {
+template <class T>
+__global__ void k_restart(int n, int m, int to_average, int adaptive, T* __restrict__ x, T* __restrict__ y,
+                          T* __restrict__ x_bar, const T* __restrict__ x_avg, const T* __restrict__ y_avg,
+                          T* __restrict__ ax, T* __restrict__ ax_prev, const T* __restrict__ ax_avg,
+                          T* __restrict__ x_sum, T* __restrict__ y_sum, T* __restrict__ x_restart,
+                          T* __restrict__ y_restart, PdlpState* st) {
     const int stride = blockDim.x * gridDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
-        double xj = x[j];
+        T xj = x[j];
         if (to_average) { xj = x_avg[j]; x[j] = xj; }
         x_bar[j] = xj;
-        x_sum[j] = 0.0;
+        x_sum[j] = T(0);
         x_restart[j] = xj;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-        double yi = y[i];
+        T yi = y[i];
         if (to_average) { yi = y_avg[i]; y[i] = yi; }
-        y_sum[i] = 0.0;
+        y_sum[i] = T(0);
         y_restart[i] = yi;
         if (adaptive) {
-            double a = ax[i];
+            T a = ax[i];
             if (to_average) { a = ax_avg[i]; ax[i] = a; }
             ax_prev[i] = a;
         }
@@ -391,7 +428,8 @@ __global__ void k_set_omega(PdlpState* st, double omega, double terms_fixed) {
 // ----------------------------------------------------------- norms / power it.
 
 // Sum of squares of v over finite entries below 1e30 in magnitude (block partials).
-__global__ void k_sumsq(const double* __restrict__ v, int n, int finite_only, double* __restrict__ partial) {
+template <class T>
+__global__ void k_sumsq(const T* __restrict__ v, int n, int finite_only, double* __restrict__ partial) {
     __shared__ double smem[kWarps];
     Slots<1, 1u> acc;
     acc.init();
@@ -493,7 +531,8 @@ __global__ void k_round_pow2(double* __restrict__ s, int n) {
     }
 }
 
-__global__ void k_fill_d(double* __restrict__ v, double value, int n) {
+template <class T>
+__global__ void k_fill_v(T* __restrict__ v, T value, int n) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x) v[j] = value;
 }
 
@@ -545,6 +584,22 @@ __global__ void k_to_scaled(int n, int m, const double* __restrict__ Cs, const d
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y[i] = y[i] / R[i];
 }
 
+// FP64 point from the FP32 phase: x^ = x, y^ = y (bounds kept exactly).
+__global__ void k_widen(int n, int m, const float* __restrict__ x32, const float* __restrict__ y32,
+                        const double* __restrict__ cl, const double* __restrict__ cu, double* __restrict__ x,
+                        double* __restrict__ y) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
+        x[j] = fmin(fmax(static_cast<double>(x32[j]), cl[j]), cu[j]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y[i] = static_cast<double>(y32[i]);
+}
+
+__global__ void k_narrow(long long n, const double* __restrict__ in, float* __restrict__ out) {
+    for (long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; j < n;
+         j += static_cast<long long>(blockDim.x) * gridDim.x)
+        out[j] = static_cast<float>(in[j]);
+}
+
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -568,24 +623,20 @@ Kkt to_kkt(const double* r, double cost_norm, double bound_norm) {
     return k;
 }
 
-struct PdlpRun {
+inline int eg(int len) { return elem_grid(std::max(len, 1)); }
+
+// ------------------------------------------------------------- FP64 model
+
+// The scaled FP64 model: factors, scaled values of A and A^T, scaled vectors,
+// and scratch for the norms and ||A||_2.
+struct Scaled {
     int n = 0, m = 0, sms = 148;
     cudaStream_t stream = nullptr;
-    TileCsr A, AT;  // scaled views
+    TileCsr A, AT;  // scaled views (values owned here)
     DevBuf blob, vals;
-    double *c, *cl, *cu, *rl, *ru, *R, *Cs, *tmp_n, *tmp_m, *tmp2_m;
-    double *x, *x_cand, *x_sum, *x_avg, *x_restart, *x_bar, *aty;
-    double *y, *y_cand, *y_sum, *y_avg, *y_restart, *ax, *ax_prev, *ax_cand, *ax_avg;
-    double *part_a, *part_b, *part_c, *res, *scalar;
-    PdlpState* st;
-    double* host;
-    int grid_k2 = 1, grid_k3 = 1, grid_rr = 1, grid_rc = 1, grid_df = 1, grid_pf = 1;
+    double *c, *cl, *cu, *rl, *ru, *R, *Cs, *tmp_n, *tmp2_n, *tmp_m, *tmp2_m, *vec_n, *vec_m, *part, *scalar;
+    double* host = nullptr;
     int launches = 0;
-    std::vector<cudaGraphExec_t> graphs;
-    ~PdlpRun() {
-        for (auto g : graphs)
-            if (g) cudaGraphExecDestroy(g);
-    }
 
     int allocate(const Plan& plan) {
         n = plan.a.cols;
@@ -594,21 +645,15 @@ struct PdlpRun {
         const size_t nb = (static_cast<size_t>(n) * 8 + 255) / 256 * 256;
         const size_t mb = (static_cast<size_t>(m) * 8 + 255) / 256 * 256;
         const size_t pb = (static_cast<size_t>(sms) * 8 * 8 * 8 + 255) / 256 * 256;
-        if (blob.alloc(13 * nb + 16 * mb + 3 * pb + 4096, "cudaMalloc PDLP workspace")) return -1;
-        if (vals.alloc(static_cast<size_t>(plan.a.nnz) * 16 + 512, "cudaMalloc scaled values")) return -1;
+        if (blob.alloc(8 * nb + 7 * mb + 4 * pb + 1024, "cudaMalloc PDLP model")) return -1;
+        if (vals.alloc(static_cast<size_t>(plan.a.nnz) * 16 + 1024, "cudaMalloc scaled values")) return -1;
         char* p = blob.as<char>();
         auto take = [&](size_t b) { double* r = reinterpret_cast<double*>(p); p += b; return r; };
-        c = take(nb); cl = take(nb); cu = take(nb); Cs = take(nb); tmp_n = take(nb);
-        x = take(nb); x_cand = take(nb); x_sum = take(nb); x_avg = take(nb); x_restart = take(nb);
-        x_bar = take(nb); aty = take(nb); take(nb);
-        rl = take(mb); ru = take(mb); R = take(mb); tmp_m = take(mb); tmp2_m = take(mb);
-        y = take(mb); y_cand = take(mb); y_sum = take(mb); y_avg = take(mb); y_restart = take(mb);
-        ax = take(mb); ax_prev = take(mb); ax_cand = take(mb); ax_avg = take(mb); take(mb); take(mb);
-        part_a = take(pb); part_b = take(pb); part_c = take(pb);
-        res = take(1024);
+        c = take(nb); cl = take(nb); cu = take(nb); Cs = take(nb); tmp_n = take(nb); tmp2_n = take(nb);
+        vec_n = take(nb); take(nb);
+        rl = take(mb); ru = take(mb); R = take(mb); tmp_m = take(mb); tmp2_m = take(mb); vec_m = take(mb); take(mb);
+        part = take(4 * pb);
         scalar = take(1024);
-        st = reinterpret_cast<PdlpState*>(take(1024));
-        (void)tmp2_m;
         A = plan.a;
         AT = plan.at;
         A.val = vals.as<double>();
@@ -616,18 +661,14 @@ struct PdlpRun {
         return 0;
     }
 
-    int eg(int len) const { return elem_grid(std::max(len, 1)); }
-
     double sumsq(const double* v, int len, bool finite_only) {
         const int g = std::min(eg(len), sms * 4);
-        k_sumsq<<<g, kThreads, 0, stream>>>(v, len, finite_only ? 1 : 0, part_a);
-        k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part_a, len > 0 ? g : 0, scalar);
+        k_sumsq<double><<<g, kThreads, 0, stream>>>(v, len, finite_only ? 1 : 0, part);
+        k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part, len > 0 ? g : 0, scalar);
         launches += 2;
-        double h = 0;
         cudaMemcpyAsync(host, scalar, sizeof(double), cudaMemcpyDeviceToHost, stream);
         cudaStreamSynchronize(stream);
-        h = host[0];
-        return h;
+        return host[0];
     }
 
     // Ruiz (Scaling.cpp:11-92), then Pock-Chambolle on the Ruiz-scaled matrix,
@@ -635,26 +676,25 @@ struct PdlpRun {
     int scale(const Plan& plan, int mode, int ruiz_iters, double ruiz_tol, int* syncs) {
         const int gm = eg(m), gn = eg(n);
         const int wg_m = std::min((m + 7) / 8 + 1, sms * 16), wg_n = std::min((n + 7) / 8 + 1, sms * 16);
-        k_fill_d<<<gm, kThreads, 0, stream>>>(R, 1.0, m);
-        k_fill_d<<<gn, kThreads, 0, stream>>>(Cs, 1.0, n);
-        const bool any = (mode & (SANKHYA_B200_SCALE_RUIZ | SANKHYA_B200_SCALE_POCK_CHAMBOLLE | SANKHYA_B200_SCALE_POW2)) != 0;
+        k_fill_v<double><<<gm, kThreads, 0, stream>>>(R, 1.0, m);
+        k_fill_v<double><<<gn, kThreads, 0, stream>>>(Cs, 1.0, n);
+        const bool any = (mode & 7) != 0;
         if (any && plan.a.nnz > 0 && m > 0 && n > 0) {
             if (mode & SANKHYA_B200_SCALE_POW2) {
                 for (int pass = 0; pass < 4; ++pass) {
                     // columns first (sk_scale.c:38-47), then rows (:48-57)
                     k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 2, 1,
-                                                               tmp_n, x_avg);
-                    k_geo_update<<<gn, kThreads, 0, stream>>>(Cs, tmp_n, x_avg, n);
+                                                               tmp_n, tmp2_n);
+                    k_geo_update<<<gn, kThreads, 0, stream>>>(Cs, tmp_n, tmp2_n, n);
                     k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 2, 0,
-                                                               tmp_m, y_avg);
-                    k_geo_update<<<gm, kThreads, 0, stream>>>(R, tmp_m, y_avg, m);
+                                                               tmp_m, tmp2_m);
+                    k_geo_update<<<gm, kThreads, 0, stream>>>(R, tmp_m, tmp2_m, m);
                     launches += 4;
                 }
                 k_round_pow2<<<gm, kThreads, 0, stream>>>(R, m);
                 k_round_pow2<<<gn, kThreads, 0, stream>>>(Cs, n);
             }
             if (mode & SANKHYA_B200_SCALE_RUIZ) {
-                // factors accumulate in (R, Cs); identity restored if not converged
                 bool converged = false;
                 for (int it = 0; it < ruiz_iters; ++it) {
                     k_row_stats<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 0, 0,
@@ -662,8 +702,8 @@ struct PdlpRun {
                     k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 0, 1,
                                                                tmp_n, nullptr);
                     const int g = std::min(eg(m + n), sms * 4);
-                    k_ruiz_dev<<<g, kThreads, 0, stream>>>(tmp_m, m, tmp_n, n, part_a);
-                    k_combine<1, 0u><<<1, kThreads, 0, stream>>>(part_a, g, scalar);
+                    k_ruiz_dev<<<g, kThreads, 0, stream>>>(tmp_m, m, tmp_n, n, part);
+                    k_combine<1, 0u><<<1, kThreads, 0, stream>>>(part, g, scalar);
                     launches += 4;
                     cudaMemcpyAsync(host, scalar, sizeof(double), cudaMemcpyDeviceToHost, stream);
                     B200_TRY(cudaStreamSynchronize(stream), "Ruiz");
@@ -673,8 +713,8 @@ struct PdlpRun {
                     k_div_sqrt<<<gn, kThreads, 0, stream>>>(Cs, tmp_n, n);
                 }
                 if (!converged && !(mode & SANKHYA_B200_SCALE_POW2)) {
-                    k_fill_d<<<gm, kThreads, 0, stream>>>(R, 1.0, m);
-                    k_fill_d<<<gn, kThreads, 0, stream>>>(Cs, 1.0, n);
+                    k_fill_v<double><<<gm, kThreads, 0, stream>>>(R, 1.0, m);
+                    k_fill_v<double><<<gn, kThreads, 0, stream>>>(Cs, 1.0, n);
                 }
             }
             if (mode & SANKHYA_B200_SCALE_POCK_CHAMBOLLE) {
@@ -683,16 +723,17 @@ struct PdlpRun {
                 k_row_stats<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, Cs, R, 1, 1, tmp_n,
                                                            nullptr);
                 k_inv_sqrt_or_one<<<gm, kThreads, 0, stream>>>(tmp2_m, tmp_m, m);
-                k_inv_sqrt_or_one<<<gn, kThreads, 0, stream>>>(x_avg, tmp_n, n);
+                k_inv_sqrt_or_one<<<gn, kThreads, 0, stream>>>(tmp2_n, tmp_n, n);
                 k_mul_into<<<gm, kThreads, 0, stream>>>(R, tmp2_m, m);
-                k_mul_into<<<gn, kThreads, 0, stream>>>(Cs, x_avg, n);
+                k_mul_into<<<gn, kThreads, 0, stream>>>(Cs, tmp2_n, n);
                 launches += 6;
             }
         }
-        k_scale_values<<<wg_m, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 0,
-                                                      const_cast<double*>(A.val));
-        k_scale_values<<<wg_n, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, R, Cs, 1,
-                                                      const_cast<double*>(AT.val));
+        const int wm = std::min((m + 7) / 8 + 1, sms * 16), wn = std::min((n + 7) / 8 + 1, sms * 16);
+        k_scale_values<<<wm, kThreads, 0, stream>>>(m, plan.a.ptr, plan.a.idx, plan.a.val, R, Cs, 0,
+                                                    const_cast<double*>(A.val));
+        k_scale_values<<<wn, kThreads, 0, stream>>>(n, plan.at.ptr, plan.at.idx, plan.at.val, R, Cs, 1,
+                                                    const_cast<double*>(AT.val));
         k_scale_vectors<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, R, Cs, c, cl, cu, rl, ru);
         launches += 3;
         B200_TRY(cudaGetLastError(), "scaling launch");
@@ -702,18 +743,18 @@ struct PdlpRun {
     // GpuPdlp.cpp:179-211 on the device, one sync at the end.
     double power_norm(int iters) {
         const int g = std::min(eg(n), sms * 4);
-        k_fill_d<<<eg(n), kThreads, 0, stream>>>(x_avg, 1.0, n);
-        k_sumsq<<<g, kThreads, 0, stream>>>(x_avg, n, 0, part_a);
-        k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part_a, n > 0 ? g : 0, scalar);
-        k_normalize<<<eg(n), kThreads, 0, stream>>>(x_avg, n, scalar);
+        k_fill_v<double><<<eg(n), kThreads, 0, stream>>>(vec_n, 1.0, n);
+        k_sumsq<double><<<g, kThreads, 0, stream>>>(vec_n, n, 0, part);
+        k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part, n > 0 ? g : 0, scalar);
+        k_normalize<<<eg(n), kThreads, 0, stream>>>(vec_n, n, scalar);
         const int ga = tiled_grid<StoreEpi>(A), gt = tiled_grid<StoreEpi>(AT);
         for (int k = 0; k < iters; ++k) {
-            launch_tiled(A, x_avg, StoreEpi{ax_avg}, stream, ga);
-            launch_tiled(AT, ax_avg, StoreEpi{x_bar}, stream, gt);
-            k_sumsq<<<g, kThreads, 0, stream>>>(x_bar, n, 0, part_a);
-            k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part_a, n > 0 ? g : 0, scalar);
-            k_copy<<<eg(n), kThreads, 0, stream>>>(x_avg, x_bar, n);
-            k_normalize<<<eg(n), kThreads, 0, stream>>>(x_avg, n, scalar);
+            launch_tiled(A, vec_n, StoreEpi{vec_m}, stream, ga);
+            launch_tiled(AT, vec_m, StoreEpi{tmp_n}, stream, gt);
+            k_sumsq<double><<<g, kThreads, 0, stream>>>(tmp_n, n, 0, part);
+            k_combine<1, 1u><<<1, kThreads, 0, stream>>>(part, n > 0 ? g : 0, scalar);
+            k_copy<<<eg(n), kThreads, 0, stream>>>(vec_n, tmp_n, n);
+            k_normalize<<<eg(n), kThreads, 0, stream>>>(vec_n, n, scalar);
         }
         launches += 4 + 6 * iters;
         cudaMemcpyAsync(host, scalar, sizeof(double), cudaMemcpyDeviceToHost, stream);
@@ -722,30 +763,121 @@ struct PdlpRun {
         const double norm = std::sqrt(lambda);
         return (norm > 0.0 && std::isfinite(norm)) ? norm : 1.0;
     }
+};
 
-    void residuals(const double* xv, const double* yv, double* ax_out, double* out, int clear_accept) {
+// ------------------------------------------------------------- the iteration
+
+struct LoopParams {
+    double eps = 1e-8;
+    long long max_iterations = 0;
+    int restart_period = 64;
+    bool adaptive = true;
+    double deadline = 0.0;  // absolute time (now_s() seconds), <= 0 none
+    double matrix_norm = 1.0, eta_min_factor = 1e-6, eta_max_factor = 1e4;
+    double cost_norm = 0.0, bound_norm = 0.0;
+    double omega0 = 0.0;  // > 0: initial primal weight (else ||c|| / ||b||)
+    double eta0 = 0.0;    // > 0: initial step size (else 0.9 / ||A||_2)
+};
+
+struct LoopStats {
+    long long iterations = 0;
+    int restarts = 0, syncs = 0;
+    bool converged = false, timed_out = false, numeric = false;
+    double eta = 0.0, accept_count = 0.0, updates = 0.0, omega = 1.0;
+    Kkt best;
+};
+
+// Restarted PDLP on one problem whose data (c, bounds) and matrix views have
+// value type T; iterates of type T; reductions and decisions in FP64.
+template <class T>
+struct Core {
+    int n = 0, m = 0, sms = 148;
+    cudaStream_t stream = nullptr;
+    TileCsrT<T> A, AT;
+    const T *c = nullptr, *cl = nullptr, *cu = nullptr, *rl = nullptr, *ru = nullptr;
+    DevBuf blob;
+    T *x, *x_cand, *x_sum, *x_avg, *x_restart, *x_bar, *aty;
+    T *y, *y_cand, *y_sum, *y_avg, *y_restart, *ax, *ax_prev, *ax_cand, *ax_avg;
+    double *part_a, *part_b, *part_c, *part_d, *res;
+    PdlpState* st;
+    double* host = nullptr;
+    int grid_k2 = 1, grid_k3 = 1, grid_rr = 1, grid_rc = 1, grid_df = 1, grid_pf = 1;
+    int launches = 0;
+    std::vector<cudaGraphExec_t> graphs;
+    Core() = default;
+    Core(const Core&) = delete;
+    Core& operator=(const Core&) = delete;
+    ~Core() {
+        for (auto g : graphs)
+            if (g) cudaGraphExecDestroy(g);
+    }
+
+    int allocate(int n_, int m_, int sms_) {
+        n = n_;
+        m = m_;
+        sms = sms_;
+        const size_t nb = (static_cast<size_t>(n) * sizeof(T) + 255) / 256 * 256;
+        const size_t mb = (static_cast<size_t>(m) * sizeof(T) + 255) / 256 * 256;
+        const size_t pb = (static_cast<size_t>(sms) * 8 * 8 * 8 + 255) / 256 * 256;
+        if (blob.alloc(7 * nb + 9 * mb + 4 * pb + 2048, "cudaMalloc PDLP iterates")) return -1;
+        char* p = blob.as<char>();
+        auto take = [&](size_t b) { char* r = p; p += b; return r; };
+        x = reinterpret_cast<T*>(take(nb)); x_cand = reinterpret_cast<T*>(take(nb));
+        x_sum = reinterpret_cast<T*>(take(nb)); x_avg = reinterpret_cast<T*>(take(nb));
+        x_restart = reinterpret_cast<T*>(take(nb)); x_bar = reinterpret_cast<T*>(take(nb));
+        aty = reinterpret_cast<T*>(take(nb));
+        y = reinterpret_cast<T*>(take(mb)); y_cand = reinterpret_cast<T*>(take(mb));
+        y_sum = reinterpret_cast<T*>(take(mb)); y_avg = reinterpret_cast<T*>(take(mb));
+        y_restart = reinterpret_cast<T*>(take(mb)); ax = reinterpret_cast<T*>(take(mb));
+        ax_prev = reinterpret_cast<T*>(take(mb)); ax_cand = reinterpret_cast<T*>(take(mb));
+        ax_avg = reinterpret_cast<T*>(take(mb));
+        part_a = reinterpret_cast<double*>(take(pb)); part_b = reinterpret_cast<double*>(take(pb));
+        part_c = reinterpret_cast<double*>(take(pb)); part_d = reinterpret_cast<double*>(take(pb));
+        res = reinterpret_cast<double*>(take(1024));
+        st = reinterpret_cast<PdlpState*>(take(1024));
+        return 0;
+    }
+
+    void set_problem(const TileCsrT<T>& a, const TileCsrT<T>& at, const T* c_, const T* cl_, const T* cu_,
+                     const T* rl_, const T* ru_) {
+        A = a;
+        AT = at;
+        c = c_; cl = cl_; cu = cu_; rl = rl_; ru = ru_;
+        grid_k2 = tiled_grid<PrimalCandEpi<T>, T>(AT);
+        grid_k3 = tiled_grid<ProbeEpi<T>, T>(A);
+        grid_rr = tiled_grid<ResRowsEpi<T>, T>(A);
+        grid_rc = tiled_grid<ResColsEpi<T>, T>(AT);
+        grid_df = tiled_grid<DualFixedEpi<T>, T>(A);
+        grid_pf = tiled_grid<PrimalFixedEpi<T>, T>(AT);
+        for (auto g : graphs)
+            if (g) cudaGraphExecDestroy(g);
+        graphs.clear();
+    }
+
+    // Residual sums of (xv, yv) into out[0..13]; ax_out / aty_out optional.
+    void residuals(const T* xv, const T* yv, T* ax_out, T* aty_out, double* out, int clear_accept) {
         const int nbr = A.ntiles ? grid_rr : 0, nbc = AT.ntiles ? grid_rc : 0;
-        launch_tiled(A, xv, ResRowsEpi{yv, y_restart, rl, ru, ax_out, part_a}, stream, grid_rr);
-        launch_tiled(AT, yv, ResColsEpi{xv, x_restart, c, cl, cu, part_b}, stream, grid_rc);
+        launch_tiled(A, xv, ResRowsEpi<T>{yv, y_restart, rl, ru, ax_out, part_a}, stream, grid_rr);
+        launch_tiled(AT, yv, ResColsEpi<T>{xv, x_restart, c, cl, cu, aty_out, part_b}, stream, grid_rc);
         k_res_combine<<<1, kThreads, 0, stream>>>(part_a, nbr, part_b, nbc, out, st, clear_accept);
         launches += 3;
     }
 
     void adaptive_iteration(bool make_candidate) {
-        k_commit_dual<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, x, x_cand, x_sum, y, y_cand, y_sum, ax,
-                                                                   ax_prev, ax_cand, rl, ru, make_candidate ? 1 : 0);
+        k_commit_dual<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, x, x_cand, x_sum, y, y_cand, y_sum,
+                                                                      ax, ax_prev, ax_cand, rl, ru,
+                                                                      make_candidate ? 1 : 0);
         ++launches;
         if (!make_candidate) return;
-        launch_tiled(AT, y_cand, PrimalCandEpi{st, x, c, cl, cu, x_cand, part_c}, stream, grid_k2);
-        launch_tiled(A, x_cand,
-                     ProbeEpi{st, y, y_cand, ax, ax_cand, part_a + 4096, part_c, AT.ntiles ? grid_k2 : 0}, stream,
-                     grid_k3);
+        launch_tiled(AT, y_cand, PrimalCandEpi<T>{st, x, c, cl, cu, x_cand, part_c}, stream, grid_k2);
+        launch_tiled(A, x_cand, ProbeEpi<T>{st, y, y_cand, ax, ax_cand, part_d, part_c, AT.ntiles ? grid_k2 : 0},
+                     stream, grid_k3);
         launches += 2;
     }
 
-    void fixed_iteration(double tau, double sigma) {
-        launch_tiled(A, x_bar, DualFixedEpi{st, y, y_sum, rl, ru, sigma}, stream, grid_df);
-        launch_tiled(AT, y, PrimalFixedEpi{x, x_bar, x_sum, c, cl, cu, tau}, stream, grid_pf);
+    void fixed_iteration(T tau, T sigma) {
+        launch_tiled(A, x_bar, DualFixedEpi<T>{y, y_sum, rl, ru, sigma}, stream, grid_df);
+        launch_tiled(AT, y, PrimalFixedEpi<T>{x, x_bar, x_sum, c, cl, cu, tau}, stream, grid_pf);
         launches += 2;
     }
 
@@ -759,26 +891,143 @@ struct PdlpRun {
             B200_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
             for (int k = 0; k < period; ++k) {
                 if (adaptive) adaptive_iteration(true);
-                else fixed_iteration(tau, sigma);
+                else fixed_iteration(static_cast<T>(tau), static_cast<T>(sigma));
             }
             if (adaptive) adaptive_iteration(false);  // commit the last probe
-            residuals(x, y, nullptr, res, 0);
-            k_average<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, adaptive ? 1 : 0, x_sum, y_sum, x_avg,
-                                                                    y_avg);
-            residuals(x_avg, y_avg, ax_avg, res + 16, 1);
+            residuals(x, y, nullptr, nullptr, res, 0);
+            k_average<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, adaptive ? 1 : 0, x_sum, y_sum, x_avg,
+                                                                       y_avg);
+            residuals(x_avg, y_avg, ax_avg, nullptr, res + 16, 1);
             cudaMemcpyAsync(host, res, 32 * sizeof(double), cudaMemcpyDeviceToHost, stream);
             B200_TRY(cudaStreamEndCapture(stream, &g), "end capture");
             cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return fail_cuda("graph instantiate", e);
-            graphs.push_back(exec);
-            *graph_slot = static_cast<int>(graphs.size()) - 1;
+            if (*graph_slot >= 0) {
+                graphs[static_cast<size_t>(*graph_slot)] = exec;
+            } else {
+                graphs.push_back(exec);
+                *graph_slot = static_cast<int>(graphs.size()) - 1;
+            }
             launches = saved;
         }
         B200_TRY(cudaGraphLaunch(exec, stream), "graph launch");
         launches += (adaptive ? 3 * period + 1 : 2 * period) + 7;
         return 0;
     }
+
+    // Starting point already in x, y (T). Sets up A x, the restart reference
+    // and the step state, then runs restarted windows (GpuPdlp.cpp:252-534).
+    int run(const LoopParams& lp, LoopStats* out, const Plan* plan) {
+        const size_t nb = sizeof(T) * static_cast<size_t>(std::max(n, 1));
+        const size_t mb = sizeof(T) * static_cast<size_t>(std::max(m, 1));
+        for (T* v : {x_sum, x_cand, x_avg, aty}) cudaMemsetAsync(v, 0, nb, stream);
+        for (T* v : {y_sum, y_cand, y_avg, ax_cand, ax_avg}) cudaMemsetAsync(v, 0, mb, stream);
+        B200_TRY(cudaMemcpyAsync(x_restart, x, nb, cudaMemcpyDeviceToDevice, stream), "copy");
+        B200_TRY(cudaMemcpyAsync(x_bar, x, nb, cudaMemcpyDeviceToDevice, stream), "copy");
+        B200_TRY(cudaMemcpyAsync(y_restart, y, mb, cudaMemcpyDeviceToDevice, stream), "copy");
+        if (m) launch_tiled(A, x, StoreEpiT<T>{ax}, stream, tiled_grid<StoreEpiT<T>, T>(A));
+        B200_TRY(cudaMemcpyAsync(ax_prev, ax, mb, cudaMemcpyDeviceToDevice, stream), "copy");
+        const double eta_global = kStepSafety / lp.matrix_norm;
+        const double eta_min = lp.eta_min_factor / lp.matrix_norm, eta_max = lp.eta_max_factor / lp.matrix_norm;
+        double omega = 1.0;
+        if (lp.cost_norm > 0.0 && lp.bound_norm > 0.0)
+            omega = std::min(kMaxWeight, std::max(kMinWeight, lp.cost_norm / lp.bound_norm));
+        if (lp.omega0 > 0.0) omega = lp.omega0;
+        const double eta_start = lp.eta0 > 0.0 ? std::min(std::max(lp.eta0, eta_min), eta_max) : eta_global;
+        k_init_state<<<1, 1, 0, stream>>>(st, eta_start, omega, eta_min, eta_max);
+        B200_TRY(cudaGetLastError(), "PDLP setup");
+
+        long long iteration = 0;
+        int windows_since_restart = 0;
+        long long iterations_since_restart = 0;
+        double mu_at_restart = std::numeric_limits<double>::infinity(), mu_previous = mu_at_restart;
+        int slot_full = -1, slot_tail = -1;
+        double omega_full = -1.0, omega_tail = -1.0;
+        while (iteration < lp.max_iterations) {
+            const int period = static_cast<int>(std::min<long long>(lp.restart_period, lp.max_iterations - iteration));
+            if (period <= 0) break;
+            const double terms_fixed = static_cast<double>((windows_since_restart + 1) * lp.restart_period);
+            k_set_omega<<<1, 1, 0, stream>>>(st, omega, terms_fixed);
+            const double tau = eta_global / omega, sigma = eta_global * omega;
+            const bool full = period == lp.restart_period;
+            int* slot = full ? &slot_full : &slot_tail;
+            double* baked = full ? &omega_full : &omega_tail;
+            if (!lp.adaptive && *slot >= 0 && omega != *baked) {
+                // the fixed path bakes tau/sigma into the graph: rebuild it when omega moved
+                cudaGraphExecDestroy(graphs[static_cast<size_t>(*slot)]);
+                graphs[static_cast<size_t>(*slot)] = nullptr;
+            }
+            *baked = omega;
+            if (window(period, lp.adaptive, tau, sigma, slot)) return -1;
+            B200_TRY(cudaStreamSynchronize(stream), "PDLP window");
+            ++out->syncs;
+            if (plan && plan->d_err) {
+                unsigned int word = 0;
+                if (cudaMemcpy(&word, plan->d_err, sizeof(word), cudaMemcpyDeviceToHost) == cudaSuccess && word) {
+                    cudaMemset(plan->d_err, 0, sizeof(word));
+                    return fail_msg("device wait gave up");
+                }
+            }
+            iteration += period;
+            iterations_since_restart += period;
+            ++windows_since_restart;
+            const double* h = host;
+            const Kkt current = to_kkt(h, lp.cost_norm, lp.bound_norm);
+            const Kkt average = to_kkt(h + 16, lp.cost_norm, lp.bound_norm);
+            out->eta = h[16 + 8];
+            out->accept_count = h[16 + 9];
+            out->updates = h[16 + 10];
+            const bool average_better = average.worst() < current.worst();
+            out->best = average_better ? average : current;
+            const Kkt best = out->best;
+            if (!std::isfinite(current.primal) && !std::isfinite(average.primal)) {
+                out->numeric = true;
+                break;
+            }
+            if (best.primal <= lp.eps && best.dual <= lp.eps && best.gap <= lp.eps) {
+                if (average_better) {
+                    B200_TRY(cudaMemcpyAsync(x, x_avg, nb, cudaMemcpyDeviceToDevice, stream), "copy");
+                    B200_TRY(cudaMemcpyAsync(y, y_avg, mb, cudaMemcpyDeviceToDevice, stream), "copy");
+                }
+                out->converged = true;
+                break;
+            }
+            if (lp.deadline > 0.0 && now_s() > lp.deadline) {
+                out->timed_out = true;
+                break;
+            }
+            const double mu = best.worst();
+            const bool sufficient = mu <= kSufficient * mu_at_restart;
+            const bool necessary = mu <= kNecessary * mu_at_restart && mu > mu_previous;
+            const bool artificial =
+                static_cast<double>(iterations_since_restart) >= kArtificial * static_cast<double>(iteration);
+            mu_previous = mu;
+            if (!(sufficient || necessary || artificial)) continue;
+            k_restart<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(
+                n, m, average_better ? 1 : 0, lp.adaptive ? 1 : 0, x, y, x_bar, x_avg, y_avg, ax, ax_prev, ax_avg,
+                x_sum, y_sum, x_restart, y_restart, st);
+            ++launches;
+            windows_since_restart = 0;
+            iterations_since_restart = 0;
+            mu_at_restart = mu;
+            mu_previous = std::numeric_limits<double>::infinity();
+            ++out->restarts;
+            if (best.pmove > 1e-14 && best.dmove > 1e-14) {
+                const double target = best.dmove / best.pmove;
+                const double updated = std::exp(kSmoothing * std::log(target) + (1.0 - kSmoothing) * std::log(omega));
+                if (std::isfinite(updated)) omega = std::min(kMaxWeight, std::max(kMinWeight, updated));
+            }
+        }
+        out->iterations += iteration;
+        out->omega = omega;
+        return 0;
+    }
+};
+
+struct HostSlot {
+    double* p = nullptr;
+    ~HostSlot() { if (p) cudaFreeHost(p); }
 };
 
 }  // namespace
@@ -838,176 +1087,157 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     const double t_start = now_s();
     std::shared_ptr<Plan> plan;
     if (get_plan(matrix, &plan)) return -1;
-    PdlpRun run;
-    run.stream = engine_stream();
-    if (run.allocate(*plan)) return -1;
-    struct HostSlot {
-        double* p = nullptr;
-        ~HostSlot() { if (p) cudaFreeHost(p); }
-    } hs;
+    HostSlot hs;
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&hs.p), 64 * sizeof(double)), "cudaMallocHost");
-    run.host = hs.p;
-    cudaStream_t stream = run.stream;
+    cudaStream_t stream = engine_stream();
+    Scaled sc;
+    sc.stream = stream;
+    sc.host = hs.p;
+    if (sc.allocate(*plan)) return -1;
     const size_t nb = sizeof(double) * static_cast<size_t>(n), mb = sizeof(double) * static_cast<size_t>(m);
     if (n) {
-        B200_TRY(cudaMemcpyAsync(run.c, c, nb, cudaMemcpyHostToDevice, stream), "upload c");
-        B200_TRY(cudaMemcpyAsync(run.cl, col_lower, nb, cudaMemcpyHostToDevice, stream), "upload col_lower");
-        B200_TRY(cudaMemcpyAsync(run.cu, col_upper, nb, cudaMemcpyHostToDevice, stream), "upload col_upper");
+        B200_TRY(cudaMemcpyAsync(sc.c, c, nb, cudaMemcpyHostToDevice, stream), "upload c");
+        B200_TRY(cudaMemcpyAsync(sc.cl, col_lower, nb, cudaMemcpyHostToDevice, stream), "upload col_lower");
+        B200_TRY(cudaMemcpyAsync(sc.cu, col_upper, nb, cudaMemcpyHostToDevice, stream), "upload col_upper");
     }
     if (m) {
-        B200_TRY(cudaMemcpyAsync(run.rl, row_lower, mb, cudaMemcpyHostToDevice, stream), "upload row_lower");
-        B200_TRY(cudaMemcpyAsync(run.ru, row_upper, mb, cudaMemcpyHostToDevice, stream), "upload row_upper");
+        B200_TRY(cudaMemcpyAsync(sc.rl, row_lower, mb, cudaMemcpyHostToDevice, stream), "upload row_lower");
+        B200_TRY(cudaMemcpyAsync(sc.ru, row_upper, mb, cudaMemcpyHostToDevice, stream), "upload row_upper");
     }
     int syncs = 0;
-    if (run.scale(*plan, s.scaling, s.ruiz_iterations, s.ruiz_tolerance, &syncs)) return -1;
-
+    if (sc.scale(*plan, s.scaling, s.ruiz_iterations, s.ruiz_tolerance, &syncs)) return -1;
     // norms of the scaled data (GpuPdlp.cpp:94-99), finite entries only
-    const double cost_norm = std::sqrt(run.sumsq(run.c, n, true));
-    const double bl = run.sumsq(run.rl, m, true), bu = run.sumsq(run.ru, m, true);
-    const double bound_norm = std::sqrt(bl + bu);
+    const double cost_norm = std::sqrt(sc.sumsq(sc.c, n, true));
+    const double bound_norm = std::sqrt(sc.sumsq(sc.rl, m, true) + sc.sumsq(sc.ru, m, true));
     syncs += 3;
-    const double matrix_norm = run.power_norm(s.power_iterations);
+    const double matrix_norm = sc.power_norm(s.power_iterations);
     ++syncs;
-    const double eta_global = kStepSafety / matrix_norm;
-    const double eta_min = s.eta_min_factor / matrix_norm, eta_max = s.eta_max_factor / matrix_norm;
-    double omega = 1.0;
-    if (cost_norm > 0.0 && bound_norm > 0.0) omega = std::min(kMaxWeight, std::max(kMinWeight, cost_norm / bound_norm));
-
-    // initial iterate: zeros or the warm start (moved into the scaled space)
-    B200_TRY(cudaMemsetAsync(run.x, 0, std::max<size_t>(nb, 1), stream), "zero");
-    B200_TRY(cudaMemsetAsync(run.y, 0, std::max<size_t>(mb, 1), stream), "zero");
-    if (x0 && n) B200_TRY(cudaMemcpyAsync(run.x, x0, nb, cudaMemcpyHostToDevice, stream), "upload x0");
-    if (y0 && m) B200_TRY(cudaMemcpyAsync(run.y, y0, mb, cudaMemcpyHostToDevice, stream), "upload y0");
-    if (x0 || y0) k_to_scaled<<<run.eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, run.Cs, run.R, run.x, run.y);
-    for (double* v : {run.x_sum, run.x_cand, run.x_avg, run.aty}) cudaMemsetAsync(v, 0, std::max<size_t>(nb, 1), stream);
-    for (double* v : {run.y_sum, run.y_cand, run.y_avg, run.ax_cand, run.ax_avg})
-        cudaMemsetAsync(v, 0, std::max<size_t>(mb, 1), stream);
-    B200_TRY(cudaMemcpyAsync(run.x_restart, run.x, std::max<size_t>(nb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
-    B200_TRY(cudaMemcpyAsync(run.x_bar, run.x, std::max<size_t>(nb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
-    B200_TRY(cudaMemcpyAsync(run.y_restart, run.y, std::max<size_t>(mb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
-    // A x of the start point; the first extrapolation is then the identity
-    if (m) launch_tiled(run.A, run.x, StoreEpi{run.ax}, stream, tiled_grid<StoreEpi>(run.A));
-    B200_TRY(cudaMemcpyAsync(run.ax_prev, run.ax, std::max<size_t>(mb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
-    k_init_state<<<1, 1, 0, stream>>>(run.st, eta_global, omega, eta_min, eta_max);
-    B200_TRY(cudaGetLastError(), "PDLP setup");
-
-    run.grid_k2 = tiled_grid<PrimalCandEpi>(run.AT);
-    run.grid_k3 = tiled_grid<ProbeEpi>(run.A);
-    run.grid_rr = tiled_grid<ResRowsEpi>(run.A);
-    run.grid_rc = tiled_grid<ResColsEpi>(run.AT);
-    run.grid_df = tiled_grid<DualFixedEpi>(run.A);
-    run.grid_pf = tiled_grid<PrimalFixedEpi>(run.AT);
-    const bool adaptive = s.adaptive_step != 0;
-    // The probe's last-block combine needs every tile of A to launch a block.
-    if (adaptive && run.A.ntiles == 0 && m == 0) {
-        // no rows: the interaction is zero and every step is accepted; handled by the generic path
-    }
 
     TimingState& ts = timing();
     ts.last = SankhyaB200Timing{};
-    int iteration = 0, windows_since_restart = 0, iterations_since_restart = 0, restarts = 0;
-    double mu_at_restart = std::numeric_limits<double>::infinity(), mu_previous = mu_at_restart;
-    Kkt best;
-    bool converged = false, timed_out = false, numeric = false;
-    int slot_full = -1, slot_tail = -1;
-    double eta_host = eta_global, accept_count = 0, updates = 0;
-    while (iteration < s.max_iterations) {
-        const int period = std::min(s.restart_period, s.max_iterations - iteration);
-        if (period <= 0) break;
-        const double terms_fixed = static_cast<double>((windows_since_restart + 1) * s.restart_period);
-        k_set_omega<<<1, 1, 0, stream>>>(run.st, omega, terms_fixed);
-        const double tau = eta_global / omega, sigma = eta_global * omega;
-        // the fixed path bakes tau/sigma into the graph: rebuild it when omega moves
-        int* slot = period == s.restart_period ? &slot_full : &slot_tail;
-        if (!adaptive && *slot >= 0) {
-            cudaGraphExecDestroy(run.graphs[static_cast<size_t>(*slot)]);
-            run.graphs[static_cast<size_t>(*slot)] = nullptr;
+    LoopStats stats;
+    LoopParams lp;
+    lp.restart_period = s.restart_period;
+    lp.adaptive = s.adaptive_step != 0;
+    lp.deadline = s.time_limit > 0.0 ? t_start + s.time_limit : 0.0;
+    lp.matrix_norm = matrix_norm;
+    lp.eta_min_factor = s.eta_min_factor;
+    lp.eta_max_factor = s.eta_max_factor;
+    int refinements = 0;
+    int launches = sc.launches;
+
+    // FP64 point of the scaled problem (x^, y^): starts at zeros or the warm start
+    Core<double> hi;
+    hi.stream = stream;
+    hi.host = hs.p;
+    if (hi.allocate(n, m, sc.sms)) return -1;
+    hi.set_problem(sc.A, sc.AT, sc.c, sc.cl, sc.cu, sc.rl, sc.ru);
+    B200_TRY(cudaMemsetAsync(hi.x, 0, std::max<size_t>(nb, 1), stream), "zero");
+    B200_TRY(cudaMemsetAsync(hi.y, 0, std::max<size_t>(mb, 1), stream), "zero");
+    if (x0 && n) B200_TRY(cudaMemcpyAsync(hi.x, x0, nb, cudaMemcpyHostToDevice, stream), "upload x0");
+    if (y0 && m) B200_TRY(cudaMemcpyAsync(hi.y, y0, mb, cudaMemcpyHostToDevice, stream), "upload y0");
+    if (x0 || y0) k_to_scaled<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, sc.Cs, sc.R, hi.x, hi.y);
+
+    if (s.precision == SANKHYA_B200_FP64) {
+        lp.eps = s.eps_optimal;
+        lp.max_iterations = s.max_iterations;
+        lp.cost_norm = cost_norm;
+        lp.bound_norm = bound_norm;
+        if (hi.run(lp, &stats, plan.get())) return -1;
+        launches += hi.launches;
+    } else {
+        // -------------------------------------- FP32 iterations, then an FP64 finish
+        DevBuf vals32, blob32;
+        const size_t nnz = static_cast<size_t>(plan->a.nnz);
+        if (vals32.alloc(nnz * 8 + 1024, "cudaMalloc FP32 values")) return -1;
+        float* a32 = vals32.as<float>();
+        float* at32 = a32 + (nnz + 63) / 64 * 64;
+        k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.A.val, a32);
+        k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.AT.val, at32);
+        const size_t nf = (static_cast<size_t>(n) * 4 + 255) / 256 * 256;
+        const size_t mf = (static_cast<size_t>(m) * 4 + 255) / 256 * 256;
+        if (blob32.alloc(3 * nf + 2 * mf + 256, "cudaMalloc FP32 model")) return -1;
+        char* base = blob32.as<char>();
+        float* c32 = reinterpret_cast<float*>(base);
+        float* cl32 = reinterpret_cast<float*>(base + nf);
+        float* cu32 = reinterpret_cast<float*>(base + 2 * nf);
+        float* rl32 = reinterpret_cast<float*>(base + 3 * nf);
+        float* ru32 = reinterpret_cast<float*>(base + 3 * nf + mf);
+        const int gv = eg(std::max(n, m));
+        k_narrow<<<gv, kThreads, 0, stream>>>(n, sc.c, c32);
+        k_narrow<<<gv, kThreads, 0, stream>>>(n, sc.cl, cl32);
+        k_narrow<<<gv, kThreads, 0, stream>>>(n, sc.cu, cu32);
+        k_narrow<<<gv, kThreads, 0, stream>>>(m, sc.rl, rl32);
+        k_narrow<<<gv, kThreads, 0, stream>>>(m, sc.ru, ru32);
+        Core<float> lo;
+        lo.stream = stream;
+        lo.host = hs.p;
+        if (lo.allocate(n, m, sc.sms)) return -1;
+        lo.set_problem(sc.A.with_values<float>(a32), sc.AT.with_values<float>(at32), c32, cl32, cu32, rl32, ru32);
+        k_narrow<<<gv, kThreads, 0, stream>>>(n, hi.x, lo.x);
+        k_narrow<<<gv, kThreads, 0, stream>>>(m, hi.y, lo.y);
+        LoopParams flp = lp;
+        flp.eps = std::max(s.eps_optimal, 1e-4);
+        flp.max_iterations = s.max_iterations;
+        flp.cost_norm = cost_norm;
+        flp.bound_norm = bound_norm;
+        LoopStats fs;
+        if (lo.run(flp, &fs, plan.get())) return -1;
+        stats = fs;
+        k_widen<<<gv, kThreads, 0, stream>>>(n, m, lo.x, lo.y, sc.cl, sc.cu, hi.x, hi.y);
+        const long long left = s.max_iterations - fs.iterations;
+        if (!fs.numeric && !fs.timed_out && left > 0 && (!fs.converged || s.eps_optimal < flp.eps)) {
+            lp.eps = s.eps_optimal;
+            lp.max_iterations = left;
+            lp.cost_norm = cost_norm;
+            lp.bound_norm = bound_norm;
+            lp.omega0 = fs.omega;
+            lp.eta0 = fs.eta;
+            LoopStats fin;
+            if (hi.run(lp, &fin, plan.get())) return -1;
+            ++refinements;
+            stats.iterations += fin.iterations;
+            stats.restarts += fin.restarts;
+            stats.updates += fin.updates;
+            stats.accept_count += fin.accept_count;
+            stats.syncs += fin.syncs;
+            stats.eta = fin.eta;
+            stats.omega = fin.omega;
+            stats.best = fin.best;
+            stats.converged = fin.converged;
+            stats.timed_out = fin.timed_out;
+            stats.numeric = fin.numeric;
         }
-        if (run.window(period, adaptive, tau, sigma, slot)) return -1;
-        B200_TRY(cudaStreamSynchronize(stream), "PDLP window");
-        ++syncs;
-        {
-            unsigned int word = 0;
-            if (plan->d_err && cudaMemcpy(&word, plan->d_err, sizeof(word), cudaMemcpyDeviceToHost) == cudaSuccess &&
-                word != 0) {
-                cudaMemset(plan->d_err, 0, sizeof(word));
-                return fail_msg("device wait for a tile copy gave up");
-            }
-        }
-        iteration += period;
-        iterations_since_restart += period;
-        ++windows_since_restart;
-        const double* h = run.host;
-        const Kkt current = to_kkt(h, cost_norm, bound_norm);
-        const Kkt average = to_kkt(h + 16, cost_norm, bound_norm);
-        eta_host = h[16 + 8];
-        accept_count = h[16 + 9];
-        updates = h[16 + 10];
-        const bool average_better = average.worst() < current.worst();
-        best = average_better ? average : current;
-        if (!std::isfinite(current.primal) && !std::isfinite(average.primal)) {
-            numeric = true;
-            break;
-        }
-        if (best.primal <= s.eps_optimal && best.dual <= s.eps_optimal && best.gap <= s.eps_optimal) {
-            if (average_better) {
-                B200_TRY(cudaMemcpyAsync(run.x, run.x_avg, std::max<size_t>(nb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
-                B200_TRY(cudaMemcpyAsync(run.y, run.y_avg, std::max<size_t>(mb, 1), cudaMemcpyDeviceToDevice, stream), "copy");
-            }
-            converged = true;
-            break;
-        }
-        if (s.time_limit > 0.0 && now_s() - t_start > s.time_limit) {
-            timed_out = true;
-            break;
-        }
-        const double mu = best.worst();
-        const bool sufficient = mu <= kSufficient * mu_at_restart;
-        const bool necessary = mu <= kNecessary * mu_at_restart && mu > mu_previous;
-        const bool artificial = static_cast<double>(iterations_since_restart) >= kArtificial * static_cast<double>(iteration);
-        mu_previous = mu;
-        if (!(sufficient || necessary || artificial)) continue;
-        k_restart<<<run.eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, average_better ? 1 : 0, adaptive ? 1 : 0,
-                                                                   run.x, run.y, run.x_bar, run.x_avg, run.y_avg,
-                                                                   run.ax, run.ax_prev, run.ax_avg, run.x_sum,
-                                                                   run.y_sum, run.x_restart, run.y_restart, run.st);
-        ++run.launches;
-        windows_since_restart = 0;
-        iterations_since_restart = 0;
-        mu_at_restart = mu;
-        mu_previous = std::numeric_limits<double>::infinity();
-        ++restarts;
-        if (best.pmove > 1e-14 && best.dmove > 1e-14) {
-            const double target = best.dmove / best.pmove;
-            const double updated = std::exp(kSmoothing * std::log(target) + (1.0 - kSmoothing) * std::log(omega));
-            if (std::isfinite(updated)) omega = std::min(kMaxWeight, std::max(kMinWeight, updated));
-        }
+        launches += hi.launches + lo.launches;
     }
+
     // back to the caller's space
-    k_unscale<<<run.eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, run.Cs, run.R, run.x, run.y);
-    if (n) B200_TRY(cudaMemcpyAsync(x_out, run.x, nb, cudaMemcpyDeviceToHost, stream), "download x");
-    if (y_out && m) B200_TRY(cudaMemcpyAsync(y_out, run.y, mb, cudaMemcpyDeviceToHost, stream), "download y");
+    k_unscale<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, sc.Cs, sc.R, hi.x, hi.y);
+    if (n) B200_TRY(cudaMemcpyAsync(x_out, hi.x, nb, cudaMemcpyDeviceToHost, stream), "download x");
+    if (y_out && m) B200_TRY(cudaMemcpyAsync(y_out, hi.y, mb, cudaMemcpyDeviceToHost, stream), "download y");
     B200_TRY(cudaStreamSynchronize(stream), "download");
     ++syncs;
-    result->status = numeric ? -2 : converged ? 0 : timed_out ? 2 : 1;
-    result->iterations = iteration;
-    result->restarts = restarts;
-    result->rejected_steps = adaptive ? static_cast<int>(std::max(0.0, updates - accept_count)) : 0;
+    syncs += stats.syncs;
+    const Kkt& best = stats.best;
+    result->status = stats.numeric ? -2 : stats.converged ? 0 : stats.timed_out ? 2 : 1;
+    result->iterations = static_cast<int>(std::min<long long>(stats.iterations, 2147483647LL));
+    result->restarts = stats.restarts;
+    result->rejected_steps = lp.adaptive ? static_cast<int>(std::max(0.0, stats.updates - stats.accept_count)) : 0;
     result->host_syncs = syncs;
-    result->refinements = 0;
+    result->refinements = refinements;
     result->primal_objective = best.pobj;
     result->dual_objective = best.dobj;
     result->relative_primal_residual = best.primal;
     result->relative_dual_residual = best.dual;
     result->relative_gap = best.gap;
     result->matrix_norm = matrix_norm;
-    result->final_step_size = adaptive ? eta_host : eta_global;
-    result->primal_weight = omega;
+    result->final_step_size = lp.adaptive ? stats.eta : kStepSafety / matrix_norm;
+    result->primal_weight = stats.omega;
     result->seconds = now_s() - t_start;
-    ts.last.iterations = iteration;
+    ts.last.iterations = result->iterations;
     ts.last.checkpoints = syncs;
-    ts.last.kernel_launches = run.launches;
-    return numeric ? -2 : 0;
+    ts.last.kernel_launches = launches;
+    return stats.numeric ? -2 : 0;
 }
 
 extern "C" int sankhya_b200_scale_factors(const SankhyaCudaCSR* matrix, int scaling, int ruiz_iterations,
@@ -1021,22 +1251,19 @@ extern "C" int sankhya_b200_scale_factors(const SankhyaCudaCSR* matrix, int scal
     if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) return fail_msg("no CUDA device available");
     std::shared_ptr<Plan> plan;
     if (get_plan(matrix, &plan)) return -1;
-    PdlpRun run;
-    run.stream = engine_stream();
-    if (run.allocate(*plan)) return -1;
-    struct HostSlot {
-        double* p = nullptr;
-        ~HostSlot() { if (p) cudaFreeHost(p); }
-    } hs;
+    Scaled sc;
+    sc.stream = engine_stream();
+    HostSlot hs;
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&hs.p), 64 * sizeof(double)), "cudaMallocHost");
-    run.host = hs.p;
+    sc.host = hs.p;
+    if (sc.allocate(*plan)) return -1;
     const int n = matrix->cols, m = matrix->rows;
     const size_t nb = sizeof(double) * static_cast<size_t>(n), mb = sizeof(double) * static_cast<size_t>(m);
-    B200_TRY(cudaMemsetAsync(run.blob.p, 0, run.blob.bytes, run.stream), "clear workspace");
+    B200_TRY(cudaMemsetAsync(sc.blob.p, 0, sc.blob.bytes, sc.stream), "clear workspace");
     int syncs = 0;
-    if (run.scale(*plan, scaling, ruiz_iterations, ruiz_tolerance, &syncs)) return -1;
-    if (n) B200_TRY(cudaMemcpyAsync(col_scale, run.Cs, nb, cudaMemcpyDeviceToHost, run.stream), "download C");
-    if (m) B200_TRY(cudaMemcpyAsync(row_scale, run.R, mb, cudaMemcpyDeviceToHost, run.stream), "download R");
-    B200_TRY(cudaStreamSynchronize(run.stream), "scaling");
+    if (sc.scale(*plan, scaling, ruiz_iterations, ruiz_tolerance, &syncs)) return -1;
+    if (n) B200_TRY(cudaMemcpyAsync(col_scale, sc.Cs, nb, cudaMemcpyDeviceToHost, sc.stream), "download C");
+    if (m) B200_TRY(cudaMemcpyAsync(row_scale, sc.R, mb, cudaMemcpyDeviceToHost, sc.stream), "download R");
+    B200_TRY(cudaStreamSynchronize(sc.stream), "scaling");
     return 0;
 }

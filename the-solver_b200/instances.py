@@ -20,6 +20,11 @@ the workload descriptions the engine is measured on:
   qp_config2   n=2e5, m=1e5, 10 N(0,1) entries per column of A,
                Q = diag(log-U[1e-2,1e2]) + L L^T with L having 3 N(0,0.1)
                entries per column, c~N(0,1), bounds [-5,5], rows A x0 -/+ U(0,1).
+  lp_batch_uneven  count LPs, m log-uniform in [m_lo, m_hi], n = 2m, 4-8 distinct
+               uniform rows per column, otherwise the lp_config0 recipe.
+  milp_nodes   node relaxations of one binary MILP: m=5e3, n=1e4, A >= 0 with 6
+               U[1,10] entries per column, rows <= 0.3 * row sum, c ~ -U[0,1],
+               x in [0,1]; each node fixes 1-50 random variables to 0 or 1.
 """
 from __future__ import annotations
 
@@ -161,3 +166,43 @@ def small_dense_lp(rows, cols, dense, c, rl, ru, cl, cu):
     f = lambda v: np.asarray(v, dtype=np.float64)
     return dict(m=rows, n=cols, ptr=ptr, idx=idx, val=val, c=f(c), rl=f(rl), ru=f(ru),
                 cl=f(cl), cu=f(cu), x0=np.zeros(cols))
+
+
+def lp_variable_degree(rng, m: int, n: int, deg_lo: int, deg_hi: int):
+    degrees = rng.integers(deg_lo, deg_hi + 1, size=n).astype(np.int64)
+    degrees = np.minimum(degrees, m)
+    col, row = _distinct_rows(rng, m, degrees)
+    val = rng.standard_normal(col.shape[0])
+    ptr, idx, val = _csr_from_entries(m, row, col, val)
+    return _finish_lp(rng, m, n, ptr, idx, val)
+
+
+def lp_batch_uneven(seed: int, count: int, m_lo: int = 50, m_hi: int = 5000):
+    """count independent LPs (the batched-LP workload); returns a list of instance dicts."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ms = np.exp(rng.uniform(np.log(m_lo), np.log(m_hi), size=count)).astype(np.int64)
+    return [lp_variable_degree(rng, int(m), 2 * int(m), 4, 8) for m in ms]
+
+
+def milp_nodes(seed: int, nodes: int, m: int = 5000, n: int = 10000, per_col: int = 6,
+               fix_lo: int = 1, fix_hi: int = 50):
+    """Node relaxations of one binary MILP sharing A; returns (list of instances, shared CSR)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    col, row = _distinct_rows(rng, m, np.full(n, per_col, dtype=np.int64))
+    val = rng.uniform(1.0, 10.0, size=col.shape[0])
+    ptr, idx, val = _csr_from_entries(m, row, col, val)
+    rowsum = csr_matvec(ptr, idx, val, np.ones(n))
+    base = dict(m=m, n=n, ptr=ptr, idx=idx, val=val, c=-rng.uniform(0.0, 1.0, size=n),
+                rl=np.full(m, -SK_INFINITY), ru=0.3 * rowsum, cl=np.zeros(n), cu=np.ones(n), x0=np.zeros(n))
+    out = []
+    for _ in range(nodes):
+        k = int(rng.integers(fix_lo, fix_hi + 1))
+        which = rng.choice(n, size=k, replace=False)
+        to = rng.integers(0, 2, size=k).astype(np.float64)
+        cl, cu = base["cl"].copy(), base["cu"].copy()
+        cl[which] = to
+        cu[which] = to
+        node = dict(base)
+        node["cl"], node["cu"] = cl, cu
+        out.append(node)
+    return out
