@@ -217,6 +217,30 @@ SANKHYA_CUDA_API int sankhya_b200_batch_pdhg(
     const SankhyaB200BatchSettings* settings, double* x_out, double* y_out,
     SankhyaB200BatchResult* results);
 
+/* ---------------------------------------------------- allocation-free solve */
+
+/* No counterpart in the reference. The fixed-step solve of sankhya_cuda_lp_pdhg
+   (same algorithm, arithmetic and result fields; scalar tau and sigma) for
+   callers that cannot allocate device memory while they solve: runtimes that
+   hand out all device memory from their own pool, processes with a fixed
+   device-memory budget that must not grow after start-up, services that cannot
+   take the device-wide synchronisation cudaMalloc/cudaFree can impose. It calls no cudaMalloc, cudaFree or allocating
+   library routine: the model (c, bounds) and the solution are device pointers the
+   caller owns, and the scratch (iterate buffers, reduction partials) lives in a
+   16 MiB array inside the library that every GPU loading the library holds until
+   the process exits. Limit: 4*cols + 2*rows plus about 9.5 Ki doubles of partials
+   must fit in 2 Mi doubles; larger problems are rejected with -1 and a message.
+   The matrix must come from sankhya_cuda_csr_create. The first call on a device
+   looks up the array's device address (cudaGetSymbolAddress) and must come before
+   any stream capture. All calls share the array and it keeps the last call's
+   contents: calls that overlap on the GPU race. Work is queued on the legacy
+   default stream; the call returns after the solve. */
+SANKHYA_CUDA_API int sankhya_b200_lp_pdhg_device_noalloc(
+    const SankhyaCudaCSR* matrix, const double* device_c,
+    const double* device_row_lower, const double* device_row_upper,
+    const double* device_col_lower, const double* device_col_upper,
+    SankhyaCudaLPSettings settings, double* device_solution, SankhyaCudaLPResult* result);
+
 /* Equilibration factors computed on the device, without solving: row_scale
    (rows) and col_scale (cols) such that the scaled matrix is
    diag(row_scale) A diag(col_scale). scaling is a SANKHYA_B200_SCALE_* mask:

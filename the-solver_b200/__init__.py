@@ -33,7 +33,7 @@ REFERENCE_SYMBOLS = (
 EXTENSION_SYMBOLS = (
     "sankhya_b200_set_timing", "sankhya_b200_last_timing", "sankhya_b200_pdhg_loop",
     "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve", "sankhya_b200_scale_factors",
-    "sankhya_b200_batch_default_settings", "sankhya_b200_batch_pdhg",
+    "sankhya_b200_batch_default_settings", "sankhya_b200_batch_pdhg", "sankhya_b200_lp_pdhg_device_noalloc",
 )
 
 _lib = None

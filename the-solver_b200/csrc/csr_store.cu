@@ -174,6 +174,17 @@ void unregister_plan(const void* key) {
     }
 }
 
+bool find_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out) {
+    if (m == nullptr) return false;
+    std::lock_guard<std::mutex> lock(g_registry_mutex);
+    auto it = registry().find(m->device_row_offsets);
+    if (it == registry().end() || it->second->a.rows != m->rows || it->second->a.cols != m->cols ||
+        it->second->a.nnz != m->nnz)
+        return false;
+    *out = it->second;
+    return true;
+}
+
 int get_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out) {
     if (m == nullptr) return fail_msg("null device CSR pointer");
     {

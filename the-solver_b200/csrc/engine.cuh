@@ -96,6 +96,8 @@ int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const
 // Registered plan of a handle made by sankhya_cuda_csr_create, else a plan
 // built now from the handle's device arrays (copied back to the host once).
 int get_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out);
+// Registered plan only (never builds one, never allocates); false if absent.
+bool find_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out);
 void register_plan(const void* key, std::shared_ptr<Plan> plan);
 void unregister_plan(const void* key);
 
