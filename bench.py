@@ -291,12 +291,12 @@ def run_engine(args, world, rank, local):
         (d_ms, dual_bytes(m, n, nnz), "A-side (dual) launch")
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic_lp_config1.json")
+    tpath = os.path.join(ROOT, "profiles", "traffic_lp_config1.txt")
     if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("primal" if p_ms >= d_ms else "dual")
-        except Exception:
-            traffic = None
+        figures = dict(line.strip().split("=", 1) for line in open(tpath)
+                       if "=" in line and not line.lstrip().startswith("#"))
+        key = "primal" if p_ms >= d_ms else "dual"
+        traffic = int(figures[key]) if key in figures else None
     line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
