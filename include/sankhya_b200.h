@@ -217,6 +217,22 @@ SANKHYA_CUDA_API int sankhya_b200_batch_pdhg(
     const SankhyaB200BatchSettings* settings, double* x_out, double* y_out,
     SankhyaB200BatchResult* results);
 
+/* Batched PDHG over LPs that share one matrix: the node relaxations of a
+   branch-and-bound search, which milp_solve_lp (c/src/sk_milp.c:432-459) solves
+   one at a time on the same model with new column bounds. Same loop, gates and
+   results as sankhya_b200_batch_pdhg, per LP; the matrix is read once per
+   iteration for all LPs. Arrays flagged per_lp hold batch vectors back to back
+   (LP-major: batch*n for c and column bounds, batch*m for row bounds); a zero
+   flag means one vector shared by every LP. x_out is batch*n, y_out batch*m or
+   NULL. Returns 0 or -1. */
+SANKHYA_CUDA_API int sankhya_b200_shared_batch_pdhg(
+    const SankhyaCudaCSR* matrix, int batch,
+    const double* c, int c_per_lp,
+    const double* row_lower, const double* row_upper, int row_bounds_per_lp,
+    const double* col_lower, const double* col_upper, int col_bounds_per_lp,
+    const SankhyaB200BatchSettings* settings, double* x_out, double* y_out,
+    SankhyaB200BatchResult* results);
+
 /* ---------------------------------------------------- allocation-free solve */
 
 /* No counterpart in the reference. The fixed-step solve of sankhya_cuda_lp_pdhg

@@ -33,7 +33,8 @@ REFERENCE_SYMBOLS = (
 EXTENSION_SYMBOLS = (
     "sankhya_b200_set_timing", "sankhya_b200_last_timing", "sankhya_b200_pdhg_loop",
     "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve", "sankhya_b200_scale_factors",
-    "sankhya_b200_batch_default_settings", "sankhya_b200_batch_pdhg", "sankhya_b200_lp_pdhg_device_noalloc",
+    "sankhya_b200_batch_default_settings", "sankhya_b200_batch_pdhg", "sankhya_b200_shared_batch_pdhg",
+    "sankhya_b200_lp_pdhg_device_noalloc",
 )
 
 _lib = None
@@ -181,6 +182,9 @@ def _declare(L):
         L.sankhya_b200_batch_default_settings.restype = None
         L.sankhya_b200_batch_pdhg.argtypes = [P(CSR), C.c_int, iptr, iptr, dptr, dptr, dptr, dptr, dptr,
                                               P(BatchSettings), dptr, dptr, P(BatchResult)]
+    if hasattr(L, "sankhya_b200_shared_batch_pdhg"):
+        L.sankhya_b200_shared_batch_pdhg.argtypes = [P(CSR), C.c_int, dptr, C.c_int, dptr, dptr, C.c_int, dptr,
+                                                     dptr, C.c_int, P(BatchSettings), dptr, dptr, P(BatchResult)]
 
 
 def _d(a):
@@ -367,4 +371,35 @@ def batch_pdhg(matrix: Matrix, inst, row_segments, col_segments, s: BatchSetting
     rc = lib().sankhya_b200_batch_pdhg(C.byref(matrix.handle), k, rseg.ctypes.data_as(iptr), cseg.ctypes.data_as(iptr),
                                        _p(_d(inst["c"])), _p(_d(inst["rl"])), _p(_d(inst["ru"])), _p(_d(inst["cl"])),
                                        _p(_d(inst["cu"])), C.byref(s), _p(x), _p(y), res)
+    return rc, x, y, [{f: getattr(r, f) for f, _ in BatchResult._fields_} for r in res]
+
+
+def shared_batch_pdhg(matrix: Matrix, batch: int, c, rl, ru, cl, cu, s: BatchSettings | None = None,
+                      want_dual=False):
+    """Batched sk_solve-style PDHG over LPs sharing `matrix`. Each of c, (rl, ru),
+    (cl, cu) is either one vector shared by all LPs or a (batch, len) array.
+    Returns (rc, x[batch, n], y[batch, m] or None, results list)."""
+    s = s or batch_default_settings()
+    m, n = matrix.handle.rows, matrix.handle.cols
+
+    def arr(v, length):
+        a = np.ascontiguousarray(v, dtype=np.float64)
+        per = a.ndim == 2
+        if per:
+            assert a.shape == (batch, length)
+        else:
+            assert a.shape == (length,)
+        return a, int(per)
+
+    c_, cp = arr(c, n)
+    rl_, rp = arr(rl, m)
+    ru_, rp2 = arr(ru, m)
+    cl_, kp = arr(cl, n)
+    cu_, kp2 = arr(cu, n)
+    assert rp == rp2 and kp == kp2, "lower and upper bounds must both be shared or both per LP"
+    x = np.zeros((batch, n))
+    y = np.zeros((batch, m)) if want_dual else None
+    res = (BatchResult * batch)()
+    rc = lib().sankhya_b200_shared_batch_pdhg(C.byref(matrix.handle), batch, _p(c_), cp, _p(rl_), _p(ru_), rp,
+                                              _p(cl_), _p(cu_), kp, C.byref(s), _p(x), _p(y), res)
     return rc, x, y, [{f: getattr(r, f) for f, _ in BatchResult._fields_} for r in res]

@@ -16,10 +16,9 @@
 // frozen (its iterates are carried through unchanged) and the host reads only
 // the number of LPs still running. Per LP the arithmetic is exactly the
 // single-LP loop's, so every LP's iterates equal a separate solve's bit for bit.
-#include "engine.cuh"
+#include "batch_common.cuh"
 
 #include <algorithm>
-#include <chrono>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -28,19 +27,11 @@ namespace b200 {
 
 namespace {
 
-__device__ __forceinline__ bool sk_inf(double v) { return v >= 1.0e30; }
-__device__ __forceinline__ bool sk_neg_inf(double v) { return v <= -1.0e30; }
-
-// max of non-negative doubles through their bit patterns (order-independent)
-__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, double v) {
-    if (!(v > 0.0)) {
-        if (isnan(v)) atomicMax(slot, 0x7ff8000000000000ull);
-        return;
-    }
-    atomicMax(slot, static_cast<unsigned long long>(__double_as_longlong(v)));
-}
-
-__device__ __forceinline__ double slot_value(unsigned long long b) { return __longlong_as_double(static_cast<long long>(b)); }
+using batch::atomic_max_nonneg;
+using batch::k_abs_sums;
+using batch::sk_inf;
+using batch::sk_neg_inf;
+using batch::slot_value;
 
 // sk_solve.c:901-906 with LP freezing
 struct BatchDualEpi {
@@ -161,16 +152,6 @@ __global__ void k_batch_gate(int batch, int iteration, int last, double ptol, do
     }
 }
 
-// Sequential |a| sums per CSR row in stored order (the reference's order).
-__global__ void k_abs_sums(int rows, const int* __restrict__ ptr, const double* __restrict__ val,
-                           double* __restrict__ out) {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += blockDim.x * gridDim.x) {
-        double s = 0.0;
-        for (int p = ptr[r]; p < ptr[r + 1]; ++p) s += fabs(val[p]);
-        out[r] = s;
-    }
-}
-
 __global__ void k_steps_and_max(int len, const double* __restrict__ mass, const int* __restrict__ seg,
                                 double* __restrict__ steps, unsigned long long* __restrict__ segmax) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < len; j += blockDim.x * gridDim.x) {
@@ -199,9 +180,7 @@ __global__ void k_init_box(int n, const double* __restrict__ lo, const double* _
     }
 }
 
-double now_s() {
-    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
+using batch::now_s;
 
 }  // namespace
 
