@@ -233,6 +233,53 @@ SANKHYA_CUDA_API int sankhya_b200_shared_batch_pdhg(
     const SankhyaB200BatchSettings* settings, double* x_out, double* y_out,
     SankhyaB200BatchResult* results);
 
+/* ------------------------------------------------- learned warm start */
+
+/* A bipartite message-passing network over the constraint matrix that predicts
+   a starting point (x, y) for PDLP on a parametric LP family (fixed matrix,
+   varying cost and bounds). No counterpart in the reference, which has no
+   learned component and always starts PDLP from zero (src/cuda/GpuPdlp.cpp:278-290);
+   the prediction goes to sankhya_b200_pdlp_solve as x0 / y0, cold start stays
+   the fallback, and PDLP's own relative-KKT test judges every answer.
+   Network: 16 node features, 4 rounds (settable) of width 64, bf16 tensor-core
+   dense layers with fp32 accumulation, fp32 aggregation; trained with Adam on
+   (instance, solution) pairs, one instance per step. Deterministic. */
+typedef struct SankhyaB200GnnSettings {
+    int struct_version;          /* 1 */
+    int rounds;                  /* message-passing rounds, 4 */
+    unsigned long long seed;     /* initialisation stream */
+    double learning_rate;        /* Adam step, 1e-3 */
+    double y_scale;              /* scale of the dual outputs and of their loss term, 1 */
+} SankhyaB200GnnSettings;
+
+typedef struct SankhyaB200Gnn SankhyaB200Gnn;
+
+SANKHYA_CUDA_API void sankhya_b200_gnn_default_settings(SankhyaB200GnnSettings* settings);
+SANKHYA_CUDA_API int sankhya_b200_gnn_create(const SankhyaB200GnnSettings* settings, SankhyaB200Gnn** network);
+SANKHYA_CUDA_API void sankhya_b200_gnn_destroy(SankhyaB200Gnn* network);
+SANKHYA_CUDA_API int sankhya_b200_gnn_parameter_count(const SankhyaB200Gnn* network);
+/* fp32 parameters, flat: Ev[16][64], bev, Ec[16][64], bec, per round Wc[128][64], bc,
+   Wv[128][64], bv, then wx[64], bx, wy[64], by */
+SANKHYA_CUDA_API int sankhya_b200_gnn_get_parameters(SankhyaB200Gnn* network, float* out);
+SANKHYA_CUDA_API int sankhya_b200_gnn_set_parameters(SankhyaB200Gnn* network, const float* in);
+/* x_out (cols, inside the column bounds) and y_out (rows, may be NULL). */
+SANKHYA_CUDA_API int sankhya_b200_gnn_predict(
+    SankhyaB200Gnn* network, const SankhyaCudaCSR* matrix, const double* c,
+    const double* row_lower, const double* row_upper,
+    const double* col_lower, const double* col_upper, double* x_out, double* y_out);
+/* Loss against (x_target, y_target) and its gradient (parameter layout above). */
+SANKHYA_CUDA_API int sankhya_b200_gnn_gradient(
+    SankhyaB200Gnn* network, const SankhyaCudaCSR* matrix, const double* c,
+    const double* row_lower, const double* row_upper,
+    const double* col_lower, const double* col_upper,
+    const double* x_target, const double* y_target, double* loss, float* gradient_out);
+/* One Adam step on one instance; loss is the value before the step. */
+SANKHYA_CUDA_API int sankhya_b200_gnn_train_step(
+    SankhyaB200Gnn* network, const SankhyaCudaCSR* matrix, const double* c,
+    const double* row_lower, const double* row_upper,
+    const double* col_lower, const double* col_upper,
+    const double* x_target, const double* y_target, double* loss);
+
 /* ---------------------------------------------------- allocation-free solve */
 
 /* No counterpart in the reference. The fixed-step solve of sankhya_cuda_lp_pdhg

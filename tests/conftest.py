@@ -18,6 +18,7 @@ def _load(name, path):
 
 ENGINE = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
 INSTANCES = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+LEARNED = _load("sankhya_b200_learned", os.path.join(ROOT, "the-solver_b200", "learned.py"))
 
 
 def pytest_configure(config):
@@ -32,6 +33,11 @@ def engine():
 @pytest.fixture(scope="session")
 def instances():
     return INSTANCES
+
+
+@pytest.fixture(scope="session")
+def learned():
+    return LEARNED
 
 
 @pytest.fixture(scope="session")

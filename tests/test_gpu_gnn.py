@@ -1,0 +1,86 @@
+"""The warm-start network on the device (sankhya_b200_gnn_*): its forward pass,
+loss and gradient against the oracle's restatement with the same bf16 input
+rounding (the device accumulates in fp32, the oracle in fp64), determinism, the
+parameter interface, and what a trained network gains over cold-started PDLP on
+held-out members of a parametric family."""
+import numpy as np
+import pytest
+
+import gnn_oracle as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _instance(instances):
+    inst = dict(instances.lp_uniform(5, 60, 150, 4))
+    for k in ("cl", "cu", "ru"):
+        inst[k] = inst[k].copy()
+    inst["cu"][3] = 1e30
+    inst["cl"][4], inst["cu"][4] = -1e30, 1e30
+    inst["ru"][7] = 1e30
+    return inst
+
+
+def test_gradient_matches_oracle(engine, instances):
+    inst = _instance(instances)
+    A = engine.Matrix.from_instance(inst)
+    rng = np.random.default_rng(0)
+    xt, yt = rng.uniform(0, 10, inst["n"]), rng.standard_normal(inst["m"])
+    net = engine.Gnn(seed=7, y_scale=2.0)
+    theta = net.parameters().astype(np.float64)
+    loss, grad = net.gradient(A, inst, xt, yt)
+    ref = G.forward_backward(theta, inst, xt, yt, ys=2.0)
+    assert abs(loss - ref["loss"]) <= 1e-5 * ref["loss"]
+    assert np.linalg.norm(grad - ref["grad"]) <= 1e-4 * np.linalg.norm(ref["grad"])
+    off = 0
+    for name, shape in G.param_shapes():
+        k = int(np.prod(shape))
+        a, b = grad[off:off + k], ref["grad"][off:off + k]
+        off += k
+        assert np.linalg.norm(a - b) <= 1e-3 * max(np.linalg.norm(b), 1e-12), name
+    x, y = net.predict(A, inst)
+    assert np.max(np.abs(x - ref["x_hat"])) <= 1e-4 and np.max(np.abs(y - ref["y_hat"])) <= 1e-5
+
+
+def test_deterministic_and_parameters_roundtrip(engine, instances):
+    inst = _instance(instances)
+    A = engine.Matrix.from_instance(inst)
+    rng = np.random.default_rng(1)
+    xt, yt = rng.uniform(0, 10, inst["n"]), rng.standard_normal(inst["m"])
+    net = engine.Gnn(seed=3)
+    l1, g1 = net.gradient(A, inst, xt, yt)
+    l2, g2 = net.gradient(A, inst, xt, yt)
+    assert l1 == l2 and np.array_equal(g1, g2)
+    theta = net.parameters()
+    other = engine.Gnn(seed=99)
+    other.set_parameters(theta)
+    assert np.array_equal(other.parameters(), theta)
+    assert np.array_equal(other.gradient(A, inst, xt, yt)[1], g1)
+    bad = theta.copy()
+    bad[5] = np.nan
+    with pytest.raises(RuntimeError, match="non-finite"):
+        other.set_parameters(bad)
+
+
+def test_prediction_inside_bounds(engine, instances):
+    inst = _instance(instances)
+    A = engine.Matrix.from_instance(inst)
+    x, _ = engine.Gnn(seed=5).predict(A, inst)
+    lo = np.where(np.abs(inst["cl"]) < 1e30, inst["cl"], -np.inf)
+    hi = np.where(np.abs(inst["cu"]) < 1e30, inst["cu"], np.inf)
+    assert np.all(x >= lo) and np.all(x <= hi)
+
+
+def test_trained_network_warm_start_beats_cold_start(engine, instances, learned):
+    base = instances.lp_family_base(11, 150, 375, 4)
+    A = engine.Matrix.from_instance(base)
+    train = learned.dataset(engine, A, [instances.lp_family_member(base, 1000 + s) for s in range(64)], 1e-6)
+    assert len(train) == 64
+    net = engine.Gnn(seed=3, y_scale=learned.dual_scale(train))
+    history = learned.train(net, A, train, 40)
+    assert history[-1] < 0.25 * history[0]
+    rows = learned.evaluate(engine, net, A, [instances.lp_family_member(base, 5000 + s) for s in range(16)], 1e-6)
+    assert all(r["cold_status"] == 0 and r["warm_status"] == 0 for r in rows)
+    cold = np.mean([r["cold_iterations"] for r in rows])
+    warm = np.mean([r["warm_iterations"] for r in rows])
+    assert warm <= 0.95 * cold, (warm, cold)

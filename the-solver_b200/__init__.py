@@ -34,7 +34,10 @@ EXTENSION_SYMBOLS = (
     "sankhya_b200_set_timing", "sankhya_b200_last_timing", "sankhya_b200_pdhg_loop",
     "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve", "sankhya_b200_scale_factors",
     "sankhya_b200_batch_default_settings", "sankhya_b200_batch_pdhg", "sankhya_b200_shared_batch_pdhg",
-    "sankhya_b200_lp_pdhg_device_noalloc",
+    "sankhya_b200_lp_pdhg_device_noalloc", "sankhya_b200_gnn_default_settings", "sankhya_b200_gnn_create",
+    "sankhya_b200_gnn_destroy", "sankhya_b200_gnn_parameter_count", "sankhya_b200_gnn_get_parameters",
+    "sankhya_b200_gnn_set_parameters", "sankhya_b200_gnn_predict", "sankhya_b200_gnn_gradient",
+    "sankhya_b200_gnn_train_step",
 )
 
 _lib = None
@@ -141,6 +144,12 @@ class BatchResult(C.Structure):
                 ("anorm", C.c_double)]
 
 
+class GnnSettings(C.Structure):
+    """SankhyaB200GnnSettings."""
+    _fields_ = [("struct_version", C.c_int), ("rounds", C.c_int), ("seed", C.c_ulonglong),
+                ("learning_rate", C.c_double), ("y_scale", C.c_double)]
+
+
 SCALE_RUIZ, SCALE_POCK_CHAMBOLLE, SCALE_POW2 = 1, 2, 4
 FP64, FP32_REFINE = 0, 1
 
@@ -182,6 +191,21 @@ def _declare(L):
         L.sankhya_b200_batch_default_settings.restype = None
         L.sankhya_b200_batch_pdhg.argtypes = [P(CSR), C.c_int, iptr, iptr, dptr, dptr, dptr, dptr, dptr,
                                               P(BatchSettings), dptr, dptr, P(BatchResult)]
+    if hasattr(L, "sankhya_b200_gnn_create"):
+        L.sankhya_b200_gnn_default_settings.argtypes = [P(GnnSettings)]
+        L.sankhya_b200_gnn_default_settings.restype = None
+        L.sankhya_b200_gnn_create.argtypes = [P(GnnSettings), P(C.c_void_p)]
+        L.sankhya_b200_gnn_destroy.argtypes = [C.c_void_p]
+        L.sankhya_b200_gnn_destroy.restype = None
+        L.sankhya_b200_gnn_parameter_count.argtypes = [C.c_void_p]
+        fptr = P(C.c_float)
+        L.sankhya_b200_gnn_get_parameters.argtypes = [C.c_void_p, fptr]
+        L.sankhya_b200_gnn_set_parameters.argtypes = [C.c_void_p, fptr]
+        L.sankhya_b200_gnn_predict.argtypes = [C.c_void_p, P(CSR), dptr, dptr, dptr, dptr, dptr, dptr, dptr]
+        L.sankhya_b200_gnn_gradient.argtypes = [C.c_void_p, P(CSR), dptr, dptr, dptr, dptr, dptr, dptr, dptr,
+                                                P(C.c_double), fptr]
+        L.sankhya_b200_gnn_train_step.argtypes = [C.c_void_p, P(CSR), dptr, dptr, dptr, dptr, dptr, dptr, dptr,
+                                                  P(C.c_double)]
     if hasattr(L, "sankhya_b200_shared_batch_pdhg"):
         L.sankhya_b200_shared_batch_pdhg.argtypes = [P(CSR), C.c_int, dptr, C.c_int, dptr, dptr, C.c_int, dptr,
                                                      dptr, C.c_int, P(BatchSettings), dptr, dptr, P(BatchResult)]
@@ -403,3 +427,74 @@ def shared_batch_pdhg(matrix: Matrix, batch: int, c, rl, ru, cl, cu, s: BatchSet
     rc = lib().sankhya_b200_shared_batch_pdhg(C.byref(matrix.handle), batch, _p(c_), cp, _p(rl_), _p(ru_), rp,
                                               _p(cl_), _p(cu_), kp, C.byref(s), _p(x), _p(y), res)
     return rc, x, y, [{f: getattr(r, f) for f, _ in BatchResult._fields_} for r in res]
+
+
+
+class Gnn:
+    """The warm-start network (sankhya_b200_gnn_*): predicts (x, y) for an LP of
+    a family that shares one matrix; trained on (instance, solution) pairs."""
+
+    def __init__(self, rounds=4, seed=1, learning_rate=1e-3, y_scale=1.0):
+        st = GnnSettings()
+        lib().sankhya_b200_gnn_default_settings(C.byref(st))
+        st.rounds, st.seed, st.learning_rate, st.y_scale = rounds, seed, learning_rate, y_scale
+        self.settings = st
+        self.handle = C.c_void_p()
+        rc = lib().sankhya_b200_gnn_create(C.byref(st), C.byref(self.handle))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        self.count = lib().sankhya_b200_gnn_parameter_count(self.handle)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and _lib is not None:
+            _lib.sankhya_b200_gnn_destroy(h)
+            self.handle = None
+
+    def parameters(self):
+        out = np.zeros(self.count, dtype=np.float32)
+        if lib().sankhya_b200_gnn_get_parameters(self.handle, out.ctypes.data_as(C.POINTER(C.c_float))):
+            raise RuntimeError(last_error())
+        return out
+
+    def set_parameters(self, theta):
+        t = np.ascontiguousarray(theta, dtype=np.float32)
+        assert t.shape == (self.count,)
+        if lib().sankhya_b200_gnn_set_parameters(self.handle, t.ctypes.data_as(C.POINTER(C.c_float))):
+            raise RuntimeError(last_error())
+
+    @staticmethod
+    def _model(inst):
+        return [_d(inst[k]) for k in ("c", "rl", "ru", "cl", "cu")]
+
+    def predict(self, matrix: Matrix, inst):
+        c, rl, ru, cl, cu = self._model(inst)
+        x = np.zeros(matrix.handle.cols)
+        y = np.zeros(matrix.handle.rows)
+        rc = lib().sankhya_b200_gnn_predict(self.handle, C.byref(matrix.handle), _p(c), _p(rl), _p(ru), _p(cl), _p(cu),
+                                            _p(x), _p(y))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        return x, y
+
+    def gradient(self, matrix: Matrix, inst, x_target, y_target):
+        c, rl, ru, cl, cu = self._model(inst)
+        xt, yt = _d(x_target), _d(y_target)
+        loss = C.c_double()
+        g = np.zeros(self.count, dtype=np.float32)
+        rc = lib().sankhya_b200_gnn_gradient(self.handle, C.byref(matrix.handle), _p(c), _p(rl), _p(ru), _p(cl),
+                                             _p(cu), _p(xt), _p(yt), C.byref(loss),
+                                             g.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        return loss.value, g
+
+    def train_step(self, matrix: Matrix, inst, x_target, y_target):
+        c, rl, ru, cl, cu = self._model(inst)
+        xt, yt = _d(x_target), _d(y_target)
+        loss = C.c_double()
+        rc = lib().sankhya_b200_gnn_train_step(self.handle, C.byref(matrix.handle), _p(c), _p(rl), _p(ru), _p(cl),
+                                               _p(cu), _p(xt), _p(yt), C.byref(loss))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        return loss.value

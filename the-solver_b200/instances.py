@@ -25,6 +25,10 @@ the workload descriptions the engine is measured on:
   milp_nodes   node relaxations of one binary MILP: m=5e3, n=1e4, A >= 0 with 6
                U[1,10] entries per column, rows <= 0.3 * row sum, c ~ -U[0,1],
                x in [0,1]; each node fixes 1-50 random variables to 0 or 1.
+  lp_family    a parametric LP family on one matrix (the learned warm start's
+               workload): the lp_config0 recipe at (m, n) as the base; member s has
+               c = c0 + 0.1 N(0,1) and both bounds of row i shifted by
+               0.05 N(0,1) max(|rl_i|, |ru_i|). config 4: m=5e4, n=1e5, 10 per column.
 """
 from __future__ import annotations
 
@@ -206,3 +210,23 @@ def milp_nodes(seed: int, nodes: int, m: int = 5000, n: int = 10000, per_col: in
         node["cl"], node["cu"] = cl, cu
         out.append(node)
     return out
+
+
+def lp_family_base(seed: int, m: int, n: int, per_col: int = 10):
+    """Fixed part of a parametric family (the lp_config0 recipe at any size)."""
+    return lp_uniform(seed, m, n, per_col)
+
+
+def lp_family_member(base, seed: int):
+    """Member `seed` of the family: perturbed cost and shifted row bounds, same A."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    inst = dict(base)
+    inst["c"] = base["c"] + 0.1 * rng.standard_normal(base["n"])
+    shift = 0.05 * rng.standard_normal(base["m"]) * np.maximum(np.abs(base["rl"]), np.abs(base["ru"]))
+    inst["rl"] = base["rl"] + shift
+    inst["ru"] = base["ru"] + shift
+    return inst
+
+
+def lp_config4_base(seed: int = 4):
+    return lp_family_base(seed, 50_000, 100_000, 10)
