@@ -6,9 +6,12 @@ Workload (one GPU): LP with m = 1,000,000 rows, n = 2,000,000 columns and about
 |a| log-uniform in [1e-3, 1e3] with random signs, bounds [0, 10], rows centred on
 A x0 (the-solver_b200/instances.py: lp_config1, seed 1). FP64 throughout.
 
-A step is one call of the reference C entry point sankhya_cuda_lp_pdhg with
-max_iterations = check_every = ITERS_PER_STEP: ITERS_PER_STEP fused PDHG
-iterations plus one checkpoint evaluation, host arrays in and out.
+A step is one call of the reference C entry point
+sankhya_cuda_qp_pdhg_preconditioned (the LP case: no Hessian, per-row and
+per-column steps 0.9 / (1 + |row|_1) and 0.9 / (1 + |column|_1), as sk_solve
+chooses them) with max_iterations = check_every = ITERS_PER_STEP:
+ITERS_PER_STEP fused PDHG iterations plus one checkpoint evaluation, host
+arrays in and out.
 
   value   GB/s of algorithmic bytes, timed on the engine's stream with CUDA
           events around the iteration kernels and checkpoints (inputs resident)
@@ -239,7 +242,9 @@ def run_engine(args, world, rank, local):
     inst = I.lp_config1(SEED + rank)
     m, n, nnz = inst["m"], inst["n"], int(inst["ptr"][-1])
     gen_s = time.time() - t0
+    t0 = time.time()
     A = E.Matrix.from_instance(inst)
+    create_s = time.time() - t0
     # pinned host copies of the per-call inputs and the solution
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory().numpy()
     host = {k: pin(inst[k]) for k in ("c", "rl", "ru", "cl", "cu")}
@@ -312,7 +317,8 @@ def run_engine(args, world, rank, local):
                          "other_launch_ms": round(d_ms if p_ms >= d_ms else p_ms, 4)},
             "e2e": {"value": round(e2e, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": 8 * (4 * n + 3 * m), "d2h_bytes_per_step": 8 * n},
-            "gpu_launches": launches, "clocks": clk.summary(), "setup_s": {"generate": round(gen_s, 1)}}
+            "gpu_launches": launches, "clocks": clk.summary(), "setup_s": {"generate": round(gen_s, 1),
+                                                                                  "matrix_create": round(create_s, 3)}}
     if world == 1 and not args.no_time_to_kkt:
         line["time_to_kkt"] = time_to_kkt(E, A, inst)
     if world == 1 and not args.no_cpu_baseline:

@@ -113,6 +113,17 @@ SANKHYA_CUDA_API int sankhya_b200_pdhg_loop(
     const sk_model* model, const sk_options* options, double* x, double* y,
     double* activity, SankhyaB200LoopResult* result);
 
+/* ---------------------------------------------------------- matrix store */
+
+/* The transpose the engine keeps for a matrix made by sankhya_cuda_csr_create,
+   i.e. A in CSC form: at_ptr[cols + 1], and for each column its row indices in
+   ascending order (at_idx[nnz]) with their values (at_val[nnz]), copied to host
+   arrays. The engine builds it on the device (a stable radix sort of the entries
+   by column), replacing the host counting sorts the reference uses to move
+   between CSR and CSC (c/src/sk_solve.c csc_mv / csc_tmv order). Returns 0 or -1. */
+SANKHYA_CUDA_API int sankhya_b200_csr_transpose(const SankhyaCudaCSR* matrix, int* at_ptr, int* at_idx,
+                                                double* at_val);
+
 /* ------------------------------------------------------- restarted PDLP */
 
 enum {

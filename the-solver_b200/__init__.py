@@ -37,7 +37,7 @@ EXTENSION_SYMBOLS = (
     "sankhya_b200_lp_pdhg_device_noalloc", "sankhya_b200_gnn_default_settings", "sankhya_b200_gnn_create",
     "sankhya_b200_gnn_destroy", "sankhya_b200_gnn_parameter_count", "sankhya_b200_gnn_get_parameters",
     "sankhya_b200_gnn_set_parameters", "sankhya_b200_gnn_predict", "sankhya_b200_gnn_gradient",
-    "sankhya_b200_gnn_train_step",
+    "sankhya_b200_gnn_train_step", "sankhya_b200_csr_transpose",
 )
 
 _lib = None
@@ -191,6 +191,7 @@ def _declare(L):
         L.sankhya_b200_batch_default_settings.restype = None
         L.sankhya_b200_batch_pdhg.argtypes = [P(CSR), C.c_int, iptr, iptr, dptr, dptr, dptr, dptr, dptr,
                                               P(BatchSettings), dptr, dptr, P(BatchResult)]
+    L.sankhya_b200_csr_transpose.argtypes = [P(CSR), iptr, iptr, dptr]
     if hasattr(L, "sankhya_b200_gnn_create"):
         L.sankhya_b200_gnn_default_settings.argtypes = [P(GnnSettings)]
         L.sankhya_b200_gnn_default_settings.restype = None
@@ -498,3 +499,15 @@ class Gnn:
         if rc != 0:
             raise RuntimeError(last_error())
         return loss.value
+
+
+def csr_transpose(matrix: Matrix):
+    """The engine's stored transpose of `matrix` (A in CSC form): (ptr, idx, val)."""
+    h = matrix.handle
+    ptr = np.zeros(h.cols + 1, dtype=np.int32)
+    idx = np.zeros(max(h.nnz, 1), dtype=np.int32)
+    val = np.zeros(max(h.nnz, 1))
+    rc = lib().sankhya_b200_csr_transpose(C.byref(h), ptr.ctypes.data_as(iptr), idx.ctypes.data_as(iptr), _p(val))
+    if rc != 0:
+        raise RuntimeError(last_error())
+    return ptr, idx[:h.nnz], val[:h.nnz]

@@ -92,28 +92,24 @@ int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const
     const int rows = m->rows, cols = m->cols, nnz = m->nnz;
 
     std::vector<int> tiles_a = build_tiles(rows, h_ptr);
-    // Transpose by counting sort: rows of A visited in order, so each column
-    // of A (row of A^T) lists its row indices ascending.
+    // A^T built on the device by a stable transpose: each column of A (row of
+    // A^T) lists its row indices ascending, the order of a counting sort over the
+    // rows of A.
+    const size_t nnz_alloc = static_cast<size_t>(nnz > 0 ? nnz : 1);
+    B200_TRY(cudaMalloc(reinterpret_cast<void**>(&plan->d_at_ptr), (static_cast<size_t>(cols) + 1) * sizeof(int)),
+             "cudaMalloc A^T offsets");
+    B200_TRY(cudaMalloc(reinterpret_cast<void**>(&plan->d_at_idx), nnz_alloc * sizeof(int)), "cudaMalloc A^T indices");
+    B200_TRY(cudaMalloc(reinterpret_cast<void**>(&plan->d_at_val), nnz_alloc * sizeof(double)), "cudaMalloc A^T values");
+    if (device_transpose(rows, cols, nnz, static_cast<const int*>(m->device_row_offsets),
+                         static_cast<const int*>(m->device_column_indices), static_cast<const double*>(m->device_values),
+                         plan->d_at_ptr, plan->d_at_idx, plan->d_at_val, nullptr))
+        return -1;
     std::vector<int> at_ptr(static_cast<size_t>(cols) + 1, 0);
-    std::vector<int> at_idx(static_cast<size_t>(nnz));
-    std::vector<double> at_val(static_cast<size_t>(nnz));
-    for (int p = 0; p < nnz; ++p) at_ptr[static_cast<size_t>(h_idx[p]) + 1]++;
-    for (int j = 0; j < cols; ++j) at_ptr[j + 1] += at_ptr[j];
-    {
-        std::vector<int> next(at_ptr.begin(), at_ptr.end() - 1);
-        for (int r = 0; r < rows; ++r)
-            for (int p = h_ptr[r]; p < h_ptr[r + 1]; ++p) {
-                const int slot = next[h_idx[p]]++;
-                at_idx[slot] = r;
-                at_val[slot] = h_val[p];
-            }
-    }
+    B200_TRY(cudaMemcpy(at_ptr.data(), plan->d_at_ptr, at_ptr.size() * sizeof(int), cudaMemcpyDeviceToHost),
+             "read A^T offsets");
     std::vector<int> tiles_at = build_tiles(cols, at_ptr.data());
 
     if (upload(reinterpret_cast<void**>(&plan->d_tile_a), tiles_a.data(), tiles_a.size() * sizeof(int), "cudaMalloc tiles(A)") ||
-        upload(reinterpret_cast<void**>(&plan->d_at_ptr), at_ptr.data(), at_ptr.size() * sizeof(int), "cudaMalloc A^T offsets") ||
-        upload(reinterpret_cast<void**>(&plan->d_at_idx), at_idx.data(), at_idx.size() * sizeof(int), "cudaMalloc A^T indices") ||
-        upload(reinterpret_cast<void**>(&plan->d_at_val), at_val.data(), at_val.size() * sizeof(double), "cudaMalloc A^T values") ||
         upload(reinterpret_cast<void**>(&plan->d_tile_at), tiles_at.data(), tiles_at.size() * sizeof(int), "cudaMalloc tiles(A^T)"))
         return -1;
     B200_TRY(cudaMalloc(reinterpret_cast<void**>(&plan->d_err), sizeof(unsigned int)), "cudaMalloc error word");
@@ -332,5 +328,23 @@ extern "C" int sankhya_cuda_csr_create(SankhyaCudaCSR* matrix, int rows, int col
         return -1;
     }
     register_plan(matrix->device_row_offsets, std::move(plan));
+    return 0;
+}
+
+extern "C" int sankhya_b200_csr_transpose(const SankhyaCudaCSR* matrix, int* at_ptr, int* at_idx, double* at_val) {
+    clear_error();
+    (void)cudaGetLastError();
+    if (!matrix || !at_ptr || (matrix->nnz > 0 && (!at_idx || !at_val))) return fail_msg("invalid transpose arguments");
+    std::shared_ptr<Plan> plan;
+    if (get_plan(matrix, &plan)) return -1;
+    const TileCsr& at = plan->at;
+    B200_TRY(cudaMemcpy(at_ptr, at.ptr, (static_cast<size_t>(at.rows) + 1) * sizeof(int), cudaMemcpyDeviceToHost),
+             "read A^T offsets");
+    if (at.nnz > 0) {
+        B200_TRY(cudaMemcpy(at_idx, at.idx, static_cast<size_t>(at.nnz) * sizeof(int), cudaMemcpyDeviceToHost),
+                 "read A^T indices");
+        B200_TRY(cudaMemcpy(at_val, at.val, static_cast<size_t>(at.nnz) * sizeof(double), cudaMemcpyDeviceToHost),
+                 "read A^T values");
+    }
     return 0;
 }

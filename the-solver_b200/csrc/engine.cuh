@@ -47,6 +47,11 @@ constexpr int kShortRow = 32;          // rows up to this length: owning lane, s
 // kChunkRows rows; a row longer than kChunkNnz is a chunk of its own. Returns
 // the chunk boundaries as (row, first nonzero) pairs, ntiles + 1 of them.
 std::vector<int> build_tiles(int rows, const int* row_offsets);
+// Stable transpose of a device CSR (rows x cols, nnz): tptr[cols + 1], tidx and
+// tval receive A^T with each of its rows in ascending source-row order. Device
+// work on `stream`; returns 0 or -1 (an index outside [0, cols) is an error).
+int device_transpose(int rows, int cols, int nnz, const int* ptr, const int* idx, const double* val, int* tptr,
+                     int* tidx, double* tval, cudaStream_t stream);
 
 // A CSR with its warp-chunk schedule; T is the value type (double, or float
 // for the FP32 inner iterations of the refined PDLP).

@@ -604,50 +604,36 @@ static int solve_fixed(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessi
 
 // ================================================================ sk bridge
 
-// CSC (as stored) -> CSR with ascending columns per row (counting sort over
-// columns in order), i.e. the row order of sk_solve's scatter csc_mv.
-static void csc_to_csr(int nrow, int ncol, const int* p, const int* i, const double* x, std::vector<int>& rp,
-                       std::vector<int>& ci, std::vector<double>& cv) {
-    const int nnz = p[ncol];
-    rp.assign(static_cast<size_t>(nrow) + 1, 0);
-    ci.resize(static_cast<size_t>(nnz));
-    cv.resize(static_cast<size_t>(nnz));
-    for (int k = 0; k < nnz; ++k) rp[static_cast<size_t>(i[k]) + 1]++;
-    for (int r = 0; r < nrow; ++r) rp[r + 1] += rp[r];
-    std::vector<int> next(rp.begin(), rp.end() - 1);
-    for (int j = 0; j < ncol; ++j)
-        for (int k = p[j]; k < p[j + 1]; ++k) {
-            const int slot = next[i[k]]++;
-            ci[slot] = j;
-            cv[slot] = x[k];
-        }
-}
-
-// Device copies of a CSR and of an explicitly given transpose.
+// Device copies of a matrix given in CSC (the reference's sk_csc) and of its
+// CSR. The CSC is uploaded as stored and is the CSR of the transpose; the CSR is
+// built on the device by a stable transpose (each row's columns ascending, the
+// order of sk_solve's scatter csc_mv).
 struct OwnedPair {
     DevBuf ptr, idx, val, tiles, tptr, tidx, tval, ttiles;
     TileCsr a, at;
-    int upload(int rows, int cols, const std::vector<int>& rp, const std::vector<int>& ci, const std::vector<double>& cv,
-               const int* tp, const int* ti, const double* tv) {
-        const int nnz = rp[static_cast<size_t>(rows)];
-        std::vector<int> ta = build_tiles(rows, rp.data());
-        std::vector<int> tb = build_tiles(cols, tp);
-        if (ptr.alloc(rp.size() * 4, "cudaMalloc A") || idx.alloc(static_cast<size_t>(nnz) * 4, "cudaMalloc A") ||
-            val.alloc(static_cast<size_t>(nnz) * 8, "cudaMalloc A") || tiles.alloc(ta.size() * 4, "cudaMalloc tiles") ||
-            tptr.alloc((static_cast<size_t>(cols) + 1) * 4, "cudaMalloc A^T") ||
-            tidx.alloc(static_cast<size_t>(nnz) * 4, "cudaMalloc A^T") ||
-            tval.alloc(static_cast<size_t>(nnz) * 8, "cudaMalloc A^T") || ttiles.alloc(tb.size() * 4, "cudaMalloc tiles"))
+    int upload_csc(int rows, int cols, const int* p, const int* i, const double* x) {
+        const int nnz = p[cols];
+        const size_t nz = static_cast<size_t>(nnz > 0 ? nnz : 1);
+        std::vector<int> tb = build_tiles(cols, p);
+        if (ptr.alloc((static_cast<size_t>(rows) + 1) * 4, "cudaMalloc A") || idx.alloc(nz * 4, "cudaMalloc A") ||
+            val.alloc(nz * 8, "cudaMalloc A") || tptr.alloc((static_cast<size_t>(cols) + 1) * 4, "cudaMalloc A^T") ||
+            tidx.alloc(nz * 4, "cudaMalloc A^T") || tval.alloc(nz * 8, "cudaMalloc A^T") ||
+            ttiles.alloc(tb.size() * 4, "cudaMalloc tiles"))
             return -1;
-        B200_TRY(cudaMemcpy(ptr.p, rp.data(), ptr.bytes, cudaMemcpyHostToDevice), "upload A");
+        B200_TRY(cudaMemcpy(tptr.p, p, tptr.bytes, cudaMemcpyHostToDevice), "upload A^T");
         if (nnz) {
-            B200_TRY(cudaMemcpy(idx.p, ci.data(), idx.bytes, cudaMemcpyHostToDevice), "upload A");
-            B200_TRY(cudaMemcpy(val.p, cv.data(), val.bytes, cudaMemcpyHostToDevice), "upload A");
-            B200_TRY(cudaMemcpy(tidx.p, ti, tidx.bytes, cudaMemcpyHostToDevice), "upload A^T");
-            B200_TRY(cudaMemcpy(tval.p, tv, tval.bytes, cudaMemcpyHostToDevice), "upload A^T");
+            B200_TRY(cudaMemcpy(tidx.p, i, static_cast<size_t>(nnz) * 4, cudaMemcpyHostToDevice), "upload A^T");
+            B200_TRY(cudaMemcpy(tval.p, x, static_cast<size_t>(nnz) * 8, cudaMemcpyHostToDevice), "upload A^T");
         }
-        B200_TRY(cudaMemcpy(tiles.p, ta.data(), tiles.bytes, cudaMemcpyHostToDevice), "upload tiles");
-        B200_TRY(cudaMemcpy(tptr.p, tp, tptr.bytes, cudaMemcpyHostToDevice), "upload A^T");
         B200_TRY(cudaMemcpy(ttiles.p, tb.data(), ttiles.bytes, cudaMemcpyHostToDevice), "upload tiles");
+        if (device_transpose(cols, rows, nnz, tptr.as<int>(), tidx.as<int>(), tval.as<double>(), ptr.as<int>(),
+                             idx.as<int>(), val.as<double>(), nullptr))
+            return -1;
+        std::vector<int> rp(static_cast<size_t>(rows) + 1);
+        B200_TRY(cudaMemcpy(rp.data(), ptr.p, rp.size() * 4, cudaMemcpyDeviceToHost), "read A offsets");
+        std::vector<int> ta = build_tiles(rows, rp.data());
+        if (tiles.alloc(ta.size() * 4, "cudaMalloc tiles")) return -1;
+        B200_TRY(cudaMemcpy(tiles.p, ta.data(), tiles.bytes, cudaMemcpyHostToDevice), "upload tiles");
         a = TileCsr{rows, cols, nnz, static_cast<int>(ta.size()) / 2 - 1, ptr.as<int>(), idx.as<int>(),
                     val.as<double>(), tiles.as<int2>()};
         at = TileCsr{cols, rows, nnz, static_cast<int>(tb.size()) / 2 - 1, tptr.as<int>(), tidx.as<int>(),
@@ -667,9 +653,6 @@ static int sk_loop(const sk_model* m, const sk_options* o, double* x, double* y,
 
     // Host setup, exactly the reference's order of additions
     // (c/src/sk_solve.c:60-80 matrix_norm_bound, :863-870 diagonal test, :880-896 steps).
-    std::vector<int> rp, ci;
-    std::vector<double> cv;
-    csc_to_csr(r, n, m->A.p, m->A.i, m->A.x, rp, ci, cv);
     std::vector<double> row_mass(static_cast<size_t>(r), 0.0), col_mass(static_cast<size_t>(n), 0.0);
     std::vector<double> anorm_rows(static_cast<size_t>(r), 0.0);
     double col_max = 0.0, row_max = 0.0;
@@ -711,15 +694,10 @@ static int sk_loop(const sk_model* m, const sk_options* o, double* x, double* y,
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     OwnedPair ap;
-    if (ap.upload(r, n, rp, ci, cv, m->A.p, m->A.i, m->A.x)) return -1;
+    if (ap.upload_csc(r, n, m->A.p, m->A.i, m->A.x)) return -1;
     OwnedPair qp;
     const bool explicit_q = q && !diagonal;
-    if (explicit_q) {
-        std::vector<int> qrp, qci;
-        std::vector<double> qcv;
-        csc_to_csr(n, n, q->p, q->i, q->x, qrp, qci, qcv);
-        if (qp.upload(n, n, qrp, qci, qcv, q->p, q->i, q->x)) return -1;
-    }
+    if (explicit_q && qp.upload_csc(n, n, q->p, q->i, q->x)) return -1;
     Workspace w;
     if (w.allocate(n, r, sms * 8)) return -1;
     const size_t nb = sizeof(double) * static_cast<size_t>(n), mb = sizeof(double) * static_cast<size_t>(r);

@@ -24,13 +24,16 @@ def solve(engine, matrix, inst, eps, x0=None, y0=None, max_iterations=200_000):
     return rc, x, y, res, time.perf_counter() - t
 
 
-def dataset(engine, matrix, members, eps):
+def dataset(engine, matrix, members, eps, progress=None):
     """(member, x*, y*) for every member whose PDLP solve converged."""
     out = []
-    for inst in members:
+    for k, inst in enumerate(members):
         rc, x, y, res, _ = solve(engine, matrix, inst, eps)
         if rc == 0 and res["status"] == 0:
             out.append((inst, x, y))
+        if progress and (k + 1) % progress == 0:
+            import sys
+            print(f"solved {k + 1} / {len(members)}", file=sys.stderr, flush=True)
     return out
 
 
@@ -69,3 +72,69 @@ def evaluate(engine, gnn, matrix, members, eps, mean_x=None, mean_y=None):
             row.update(mean_iterations=mean["iterations"], mean_seconds=t_mean, mean_status=mean["status"])
         rows.append(row)
     return rows
+
+
+def _load(name, path):
+    import importlib.util
+    import sys
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def main(argv=None):
+    """Time to a relative-KKT tolerance, network warm start vs cold start, on a
+    seeded parametric family (config 4: m=50,000, n=100,000, 10 per column).
+    Prints one JSON line."""
+    import argparse
+    import json
+    import os
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    engine = _load("sankhya_b200", os.path.join(here, "__init__.py"))
+    instances = _load("sankhya_b200_instances", os.path.join(here, "instances.py"))
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--m", type=int, default=50_000)
+    ap.add_argument("--n", type=int, default=100_000)
+    ap.add_argument("--per-col", type=int, default=10)
+    ap.add_argument("--train", type=int, default=128)
+    ap.add_argument("--eval", type=int, default=16)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--eps", type=float, default=1e-6)
+    ap.add_argument("--train-eps", type=float, default=1e-6)
+    ap.add_argument("--seed", type=int, default=4)
+    a = ap.parse_args(argv)
+    base = instances.lp_family_base(a.seed, a.m, a.n, a.per_col)
+    matrix = engine.Matrix.from_instance(base)
+    t = time.perf_counter()
+    data = dataset(engine, matrix, [instances.lp_family_member(base, 1000 + s) for s in range(a.train)], a.train_eps,
+                   progress=50)
+    t_data = time.perf_counter() - t
+    net = engine.Gnn(seed=a.seed, y_scale=dual_scale(data))
+    t = time.perf_counter()
+    history = train(net, matrix, data, a.epochs)
+    t_train = time.perf_counter() - t
+    mean_x = np.mean([d[1] for d in data], axis=0)
+    mean_y = np.mean([d[2] for d in data], axis=0)
+    rows = evaluate(engine, net, matrix, [instances.lp_family_member(base, 900_000 + s) for s in range(a.eval)], a.eps,
+                    mean_x, mean_y)
+    avg = lambda k: float(np.mean([r[k] for r in rows])) if rows else None
+    out = dict(workload=f"lp_family: m={a.m}, n={a.n}, {a.per_col} per column, seed {a.seed}",
+               nnz=int(base["ptr"][-1]), eps=a.eps, train_members=len(data), train_eps=a.train_eps,
+               epochs=a.epochs, train_steps=a.epochs * len(data), data_seconds=t_data, train_seconds=t_train,
+               steps_per_second=a.epochs * len(data) / t_train, loss_first_epoch=history[0],
+               loss_last_epoch=history[-1], eval_members=len(rows),
+               converged_cold=sum(r["cold_status"] == 0 for r in rows),
+               converged_warm=sum(r["warm_status"] == 0 for r in rows),
+               cold_iterations=avg("cold_iterations"), warm_iterations=avg("warm_iterations"),
+               mean_start_iterations=avg("mean_iterations"), cold_seconds=avg("cold_seconds"),
+               warm_seconds=avg("warm_seconds"), predict_seconds=avg("predict_seconds"),
+               mean_start_seconds=avg("mean_seconds"))
+    out["speedup_warm_vs_cold"] = out["cold_seconds"] / out["warm_seconds"] if rows else None
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
