@@ -327,6 +327,8 @@ extern "C" int sankhya_b200_batch_pdhg(const SankhyaCudaCSR* matrix, int batch, 
         cur = nx;
     };
     bool timed_out = false;
+    int checks = 0;
+    batch::LoopEvents loop_events(timing().level >= 1, stream);
     while (it < s.max_iterations) {
         const int next = std::min((it / s.check_every + 1) * s.check_every, s.max_iterations);
         int k = next - it;
@@ -354,6 +356,7 @@ extern "C" int sankhya_b200_batch_pdhg(const SankhyaCudaCSR* matrix, int batch, 
         }
         it = next;
         const bool last = it >= s.max_iterations;
+        ++checks;
         B200_TRY(cudaMemsetAsync(counters, 0, 4, stream), "zero counter");
         launch_tiled(A, xb[cur], BatchRowsEpi{yb[cur], yb[cur ^ 1], drl, dru, d_rseg, done, act, viol, dstep}, stream,
                      grid_r);
@@ -370,6 +373,7 @@ extern "C" int sankhya_b200_batch_pdhg(const SankhyaCudaCSR* matrix, int batch, 
             break;
         }
     }
+    const double loop_ms = loop_events.stop(stream);
     std::vector<int> h_done(static_cast<size_t>(batch)), h_iters(static_cast<size_t>(batch));
     std::vector<double> h_report(static_cast<size_t>(batch) * 4);
     B200_TRY(cudaMemcpyAsync(x_out, xb[cur], n8, cudaMemcpyDeviceToHost, stream), "download x");
@@ -395,5 +399,7 @@ extern "C" int sankhya_b200_batch_pdhg(const SankhyaCudaCSR* matrix, int batch, 
     ts.last = SankhyaB200Timing{};
     ts.last.iterations = it;
     ts.last.kernel_launches = launches;
+    ts.last.checkpoints = checks;
+    ts.last.loop_ms = loop_ms;
     return 0;
 }

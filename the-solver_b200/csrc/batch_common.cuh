@@ -37,6 +37,29 @@ static __global__ void k_abs_sums(int rows, const int* __restrict__ ptr, const d
     }
 }
 
+// CUDA events around the iteration loop of a batched solve (timing level >= 1):
+// the device time from the first window to the last check, idle gaps included.
+struct LoopEvents {
+    cudaEvent_t a = nullptr, b = nullptr;
+    bool on = false;
+    LoopEvents(bool enabled, cudaStream_t s) : on(enabled) {
+        if (on && (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess ||
+                   cudaEventRecord(a, s) != cudaSuccess))
+            on = false;
+    }
+    double stop(cudaStream_t s) {
+        float ms = 0.f;
+        if (on && cudaEventRecord(b, s) == cudaSuccess && cudaEventSynchronize(b) == cudaSuccess)
+            cudaEventElapsedTime(&ms, a, b);
+        on = false;
+        return ms;
+    }
+    ~LoopEvents() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
 inline double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }

@@ -70,6 +70,35 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], unsigned a0, unsigned a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// Stages a 64 x 32 tile, element (r, k) = src[(r0 + r) sr + (k0 + k) sk] (zero
+// outside r0 + r < rlim, k0 + k < kend), into dst[r][k] as bf16. When k is the
+// contiguous index, a warp reads 32 consecutive k of one row. Otherwise each
+// thread takes two consecutive k of one row (lanes 0-7: eight consecutive rows,
+// lane bits 3-4: the k pair), so the global reads fill whole sectors and the
+// 4-byte shared stores of a warp fall in 32 different banks (row stride 20 words).
+template <class T>
+__device__ __forceinline__ void stage_tile(__nv_bfloat16 (*dst)[40], const T* src, long long sr, long long sk, int r0,
+                                           int rlim, int k0, int kend) {
+    if (sk == 1) {
+        for (int i = threadIdx.x; i < 64 * 32; i += kGemmThreads) {
+            const int r = i >> 5, k = i & 31;
+            const int gr = r0 + r, gk = k0 + k;
+            dst[r][k] = (gr < rlim && gk < kend) ? to_bf16(src[gr * sr + gk]) : to_bf16(0.f);
+        }
+    } else {
+        for (int q = threadIdx.x; q < 64 * 16; q += kGemmThreads) {
+            const int r = (q & 7) + 8 * ((q >> 5) & 7);
+            const int k = 2 * (((q >> 3) & 3) + 4 * (q >> 8));
+            const int gr = r0 + r, gk = k0 + k;
+            const bool live = gr < rlim;
+            __nv_bfloat162 v;
+            v.x = (live && gk < kend) ? to_bf16(src[gr * sr + gk * sk]) : to_bf16(0.f);
+            v.y = (live && gk + 1 < kend) ? to_bf16(src[gr * sr + (gk + 1) * sk]) : to_bf16(0.f);
+            *reinterpret_cast<__nv_bfloat162*>(&dst[r][k]) = v;
+        }
+    }
+}
+
 // One block = a 64 x 64 tile of C (4 warps x 16 rows, 8 n8 tiles each); K in
 // steps of 32 staged as bf16 in shared memory (A row-major, B transposed so both
 // fragments are pairs of consecutive k).
@@ -77,7 +106,7 @@ template <class TB>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(Gemm<TB> g) {
     __shared__ __align__(16) __nv_bfloat16 As[64][40];
     __shared__ __align__(16) __nv_bfloat16 Bt[64][40];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 64;
     const int kb = blockIdx.z * g.kchunk;
     const int ke = min(g.K, kb + g.kchunk);
@@ -86,26 +115,10 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(Gemm<TB> g) {
     for (int j = 0; j < 8; ++j)
 #pragma unroll
         for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
-    const bool a_k_inner = g.sak == 1;
-    const bool b_n_inner = g.sbn == 1;
     const int g4 = lane >> 2, t4 = lane & 3;
     for (int k0 = kb; k0 < ke; k0 += 32) {
-        for (int i = tid; i < 64 * 32; i += kGemmThreads) {
-            const int m = a_k_inner ? (i >> 5) : (i & 63);
-            const int k = a_k_inner ? (i & 31) : (i >> 6);
-            const int gm = m0 + m, gk = k0 + k;
-            float v = 0.f;
-            if (gm < g.M && gk < ke) v = g.A[gm * g.sam + gk * g.sak];
-            As[m][k] = to_bf16(v);
-        }
-        for (int i = tid; i < 64 * 32; i += kGemmThreads) {
-            const int n = b_n_inner ? (i & 63) : (i >> 5);
-            const int k = b_n_inner ? (i >> 6) : (i & 31);
-            const int gn = n0 + n, gk = k0 + k;
-            __nv_bfloat16 v = to_bf16(0.f);
-            if (gn < g.N && gk < ke) v = to_bf16(g.B[gk * g.sbk + gn * g.sbn]);
-            Bt[n][k] = v;
-        }
+        stage_tile(As, g.A, g.sam, g.sak, m0, g.M, k0, ke);
+        stage_tile(Bt, g.B, g.sbn, g.sbk, n0, g.N, k0, ke);
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < 32; kk += 16) {
@@ -138,13 +151,18 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(Gemm<TB> g) {
             }
 }
 
-// out[i] = sum_z part[z stride + i], z ascending.
+// out[i] = sum over z of part[z stride + i]: eight accumulators (slice z goes to
+// accumulator z mod 8, ascending z), combined by a fixed tree.
 __global__ void k_sum_slices(int count, int slices, long long stride, const float* __restrict__ part,
                              float* __restrict__ out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += blockDim.x * gridDim.x) {
-        float s = 0.f;
-        for (int z = 0; z < slices; ++z) s += part[z * stride + i];
-        out[i] = s;
+        float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int z = 0;
+        for (; z + 8 <= slices; z += 8)
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a[u] += part[(z + u) * stride + i];
+        for (int u = 0; z + u < slices; ++u) a[u] += part[(z + u) * stride + i];
+        out[i] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
     }
 }
 
@@ -217,36 +235,51 @@ struct FeatureSlots {
 
 __device__ __forceinline__ bool present(double v) { return fabs(v) < 1.0e30; }
 
-__global__ void k_feature_maxima(int m, int n, const double* __restrict__ c, const double* __restrict__ cl,
-                                 const double* __restrict__ cu, const double* __restrict__ rl,
-                                 const double* __restrict__ ru, const double* __restrict__ rnorm,
-                                 const double* __restrict__ cnorm, const int* __restrict__ aptr,
-                                 const int* __restrict__ tptr, FeatureSlots* __restrict__ s) {
+// Block maxima first (shared-memory tree), then one atomic per block and slot.
+__global__ void __launch_bounds__(kThreads) k_feature_maxima(int m, int n, const double* __restrict__ c,
+                                                             const double* __restrict__ cl, const double* __restrict__ cu,
+                                                             const double* __restrict__ rl, const double* __restrict__ ru,
+                                                             const double* __restrict__ rnorm,
+                                                             const double* __restrict__ cnorm,
+                                                             const int* __restrict__ aptr, const int* __restrict__ tptr,
+                                                             FeatureSlots* __restrict__ s) {
+    __shared__ double red[6][kThreads];
+    __shared__ unsigned int any[2];
+    if (threadIdx.x < 2) any[threadIdx.x] = 0u;
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // cmax, bmax, rmax, anorm, cdeg, rdeg
+    bool bany = false, rany = false;
     const int stride = blockDim.x * gridDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
-        atomic_max_nonneg(&s->cmax, fabs(c[j]));
-        if (present(cl[j])) {
-            atomic_max_nonneg(&s->bmax, fabs(cl[j]));
-            atomicOr(&s->bany, 1u);
-        }
-        if (present(cu[j])) {
-            atomic_max_nonneg(&s->bmax, fabs(cu[j]));
-            atomicOr(&s->bany, 1u);
-        }
-        atomic_max_nonneg(&s->anorm, cnorm[j]);
-        atomic_max_nonneg(&s->cdeg, static_cast<double>(tptr[j + 1] - tptr[j]));
+        v[0] = fmax(v[0], fabs(c[j]));
+        if (present(cl[j])) { v[1] = fmax(v[1], fabs(cl[j])); bany = true; }
+        if (present(cu[j])) { v[1] = fmax(v[1], fabs(cu[j])); bany = true; }
+        v[3] = fmax(v[3], cnorm[j]);
+        v[4] = fmax(v[4], static_cast<double>(tptr[j + 1] - tptr[j]));
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-        if (present(rl[i])) {
-            atomic_max_nonneg(&s->rmax, fabs(rl[i]));
-            atomicOr(&s->rany, 1u);
-        }
-        if (present(ru[i])) {
-            atomic_max_nonneg(&s->rmax, fabs(ru[i]));
-            atomicOr(&s->rany, 1u);
-        }
-        atomic_max_nonneg(&s->anorm, rnorm[i]);
-        atomic_max_nonneg(&s->rdeg, static_cast<double>(aptr[i + 1] - aptr[i]));
+        if (present(rl[i])) { v[2] = fmax(v[2], fabs(rl[i])); rany = true; }
+        if (present(ru[i])) { v[2] = fmax(v[2], fabs(ru[i])); rany = true; }
+        v[3] = fmax(v[3], rnorm[i]);
+        v[5] = fmax(v[5], static_cast<double>(aptr[i + 1] - aptr[i]));
+    }
+    for (int k = 0; k < 6; ++k) red[k][threadIdx.x] = v[k];
+    __syncthreads();
+    if (bany) any[0] = 1u;
+    if (rany) any[1] = 1u;
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 6; ++k) red[k][threadIdx.x] = fmax(red[k][threadIdx.x], red[k][threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomic_max_nonneg(&s->cmax, red[0][0]);
+        atomic_max_nonneg(&s->bmax, red[1][0]);
+        atomic_max_nonneg(&s->rmax, red[2][0]);
+        atomic_max_nonneg(&s->anorm, red[3][0]);
+        atomic_max_nonneg(&s->cdeg, red[4][0]);
+        atomic_max_nonneg(&s->rdeg, red[5][0]);
+        if (any[0]) atomicOr(&s->bany, 1u);
+        if (any[1]) atomicOr(&s->rany, 1u);
     }
 }
 

@@ -494,6 +494,8 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
         cur = nx;
     };
     bool timed_out = false;
+    int checks = 0;
+    batch::LoopEvents loop_events(timing().level >= 1, stream);
     while (it < s.max_iterations) {
         const int next = std::min((it / s.check_every + 1) * s.check_every, s.max_iterations);
         int k = next - it;
@@ -521,6 +523,7 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
         }
         it = next;
         const bool last = it >= s.max_iterations;
+        ++checks;
         B200_TRY(cudaMemsetAsync(counters, 0, 4, stream), "zero counter");
         if (m) {
             k_multi<<<grid_r, kThreads, 0, stream>>>(m, groups, bpi, A.ptr, A.idx, A.val, xb[cur],
@@ -541,6 +544,7 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
             break;
         }
     }
+    const double loop_ms = loop_events.stop(stream);
     std::vector<int> h_done(static_cast<size_t>(batch)), h_iters(static_cast<size_t>(batch));
     std::vector<double> h_report(static_cast<size_t>(batch) * 4);
     k_from_batch_minor<<<dim3((n + 31) / 32, bpi / 32), tblock, 0, stream>>>(n, batch, bpi, xb[cur], staging);
@@ -577,5 +581,7 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
     ts.last = SankhyaB200Timing{};
     ts.last.iterations = it;
     ts.last.kernel_launches = launches;
+    ts.last.checkpoints = checks;
+    ts.last.loop_ms = loop_ms;
     return 0;
 }

@@ -105,9 +105,26 @@ def main(argv=None):
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--train-eps", type=float, default=1e-6)
     ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="only time this many training steps (zero targets, no PDLP solves) and one prediction")
     a = ap.parse_args(argv)
     base = instances.lp_family_base(a.seed, a.m, a.n, a.per_col)
     matrix = engine.Matrix.from_instance(base)
+    if a.profile_steps:
+        net = engine.Gnn(seed=a.seed)
+        x0, y0 = np.zeros(a.n), np.zeros(a.m)
+        net.train_step(matrix, base, x0, y0)
+        t = time.perf_counter()
+        for _ in range(a.profile_steps):
+            net.train_step(matrix, base, x0, y0)
+        t_steps = time.perf_counter() - t
+        t = time.perf_counter()
+        net.predict(matrix, base)
+        print(json.dumps(dict(workload=f"lp_family: m={a.m}, n={a.n}, {a.per_col} per column, seed {a.seed}",
+                              nnz=int(base["ptr"][-1]), steps=a.profile_steps,
+                              ms_per_step=1e3 * t_steps / a.profile_steps,
+                              predict_ms=1e3 * (time.perf_counter() - t))))
+        return
     t = time.perf_counter()
     data = dataset(engine, matrix, [instances.lp_family_member(base, 1000 + s) for s in range(a.train)], a.train_eps,
                    progress=50)
