@@ -151,19 +151,30 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(Gemm<TB> g) {
             }
 }
 
-// out[i] = sum over z of part[z stride + i]: eight accumulators (slice z goes to
-// accumulator z mod 8, ascending z), combined by a fixed tree.
-__global__ void k_sum_slices(int count, int slices, long long stride, const float* __restrict__ part,
-                             float* __restrict__ out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += blockDim.x * gridDim.x) {
-        float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        int z = 0;
-        for (; z + 8 <= slices; z += 8)
+// out[i] = sum over z of part[z stride + i]. A block covers 64 consecutive
+// outputs with four slice phases (z = q mod 4); each thread keeps eight
+// accumulators (z = q + 4 u mod 32), summed by a fixed tree, and the phases are
+// combined in order: a fixed order for every output, with short load chains.
+__global__ void __launch_bounds__(4 * kH) k_sum_slices(int count, int slices, long long stride,
+                                                       const float* __restrict__ part, float* __restrict__ out) {
+    __shared__ float red[4][kH];
+    const int c = blockIdx.x * kH + (threadIdx.x & (kH - 1)), q = threadIdx.x >> 6;
+    float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (c < count)
+        for (int z0 = q; z0 < slices; z0 += 32)
 #pragma unroll
-            for (int u = 0; u < 8; ++u) a[u] += part[(z + u) * stride + i];
-        for (int u = 0; z + u < slices; ++u) a[u] += part[(z + u) * stride + i];
-        out[i] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+            for (int u = 0; u < 8; ++u)
+                if (z0 + 4 * u < slices) a[u] += part[(z0 + 4 * u) * stride + c];
+    red[q][threadIdx.x & (kH - 1)] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    __syncthreads();
+    if (q == 0 && c < count) {
+        const int i = threadIdx.x;
+        out[c] = (red[0][i] + red[1][i]) + (red[2][i] + red[3][i]);
     }
+}
+
+void sum_slices(int count, int slices, long long stride, const float* part, float* out, cudaStream_t st) {
+    k_sum_slices<<<(count + kH - 1) / kH, 4 * kH, 0, st>>>(count, slices, stride, part, out);
 }
 
 // --------------------------------------------------------- aggregation
@@ -590,13 +601,13 @@ void gemm_weight_grad(SankhyaB200Gnn* s, cudaStream_t st, int rows, const float*
     const int chunk = (rows + slices - 1) / slices;
     Gemm<float> g{K, kH, rows, X, 1, ldx, dz, kH, 1, s->part, kH, 1, static_cast<long long>(K) * kH, chunk, nullptr, 0};
     k_gemm_bf16<float><<<dim3((K + 63) / 64, 1, slices), kGemmThreads, 0, st>>>(g);
-    k_sum_slices<<<elem_blocks(K * kH), kThreads, 0, st>>>(K * kH, slices, static_cast<long long>(K) * kH, s->part, out);
+    sum_slices(K * kH, slices, static_cast<long long>(K) * kH, s->part, out, st);
 }
 
 void bias_grad(SankhyaB200Gnn* s, cudaStream_t st, int rows, const float* dz, float* out) {
     const int blocks = kRedBlocks;
     k_colsum64<<<blocks, 4 * kH, 0, st>>>(rows, dz, s->part);
-    k_sum_slices<<<1, kH, 0, st>>>(kH, blocks, kH, s->part, out);
+    sum_slices(kH, blocks, kH, s->part, out, st);
 }
 
 void spmm(cudaStream_t st, const TileCsr& M, const float* in, int sin, const float* pre, const float* post, float* out,
@@ -651,16 +662,16 @@ void heads(SankhyaB200Gnn* g, const Plan& plan, cudaStream_t st, bool with_targe
                 with_target ? g->x_t : nullptr, g->gv, kX, g->part};
     k_head<<<blocks, kThreads, 0, st>>>(hx);
     if (with_target) {
-        k_sum_slices<<<1, kH + 2, 0, st>>>(kH + 1, blocks, kH + 2, g->part, g->grad + o.wx);
-        k_sum_slices<<<1, 1, 0, st>>>(1, blocks, kH + 2, g->part + kH + 1, g->lossf);
+        sum_slices(kH + 1, blocks, kH + 2, g->part, g->grad + o.wx, st);
+        sum_slices(1, blocks, kH + 2, g->part + kH + 1, g->lossf, st);
     }
     if (m) {
         HeadArgs hy{m, g->xc[R], kX, g->params + o.wy, nullptr, nullptr, nullptr, g->settings.y_scale, 0, g->y_hat,
                     with_target ? g->y_t : nullptr, g->gc, kX, g->part};
         k_head<<<blocks, kThreads, 0, st>>>(hy);
         if (with_target) {
-            k_sum_slices<<<1, kH + 2, 0, st>>>(kH + 1, blocks, kH + 2, g->part, g->grad + o.wy);
-            k_sum_slices<<<1, 1, 0, st>>>(1, blocks, kH + 2, g->part + kH + 1, g->lossf + 1);
+            sum_slices(kH + 1, blocks, kH + 2, g->part, g->grad + o.wy, st);
+            sum_slices(1, blocks, kH + 2, g->part + kH + 1, g->lossf + 1, st);
         }
     } else if (with_target) {
         cudaMemsetAsync(g->grad + o.wy, 0, sizeof(float) * (kH + 1), st);
