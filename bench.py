@@ -401,6 +401,48 @@ def run_batches(args):
     return 0
 
 
+def run_qp(args):
+    """Convex QP workload (not the headline line): n = 200,000, m = 100,000, A with 10
+    N(0,1) entries per column, Q = diag(log-U[1e-2, 1e2]) + L L^T (L: 3 N(0, 0.1)
+    entries per column), bounds [-5, 5], rows x0 -/+ U(0,1). Device time per PDHG
+    iteration of the diagonal-proximal path (sankhya_cuda_diagonal_qp_pdhg, Q's
+    diagonal D) and of the general sparse-Hessian path (sankhya_cuda_sparse_qp_pdhg,
+    explicit Q = D + L L^T: one more fused product per iteration). Prints one JSON line."""
+    E = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
+    I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    inst = I.qp_config2(2)
+    m, n, nnz = inst["m"], inst["n"], int(inst["ptr"][-1])
+    qnnz = int(inst["q_ptr"][-1])
+    A = E.Matrix.from_instance(inst)
+    Q = E.Matrix.from_instance(inst, hessian=True)
+    its = 400
+    s = E.settings(its, its, 0.005, 0.5, 1.0, 1e-300)   # tau |Q| < 1, tau sigma |A|^2 < 1
+    paths = {"diagonal": dict(qdiag=inst["qdiag"]), "sparse_hessian": dict(hessian=Q)}
+    extra = {"diagonal": 8 * n, "sparse_hessian": 12 * qnnz + 4 * (n + 1) + 8 * n + 16 * n}
+    out = {"metric": "QP PDHG device time per iteration", "unit": "us", "higher_is_better": False,
+           "data": "synthetic", "dtype": "f64",
+           "workload": f"qp_config2: n={n}, m={m}, nnz(A)={nnz}, nnz(Q)={qnnz}, Q = D + L L^T"}
+    peak, _ = measured_peak()
+    for name, kw in paths.items():
+        E.set_timing(1)
+        E.pdhg(A, inst, s, **kw)
+        best = None
+        for _ in range(3):
+            rc, x, y, r = E.pdhg(A, inst, s, **kw)
+            if rc != 0:
+                raise RuntimeError(f"{name}: {E.last_error()}")
+            t = E.last_timing()
+            per = 1e3 * (t["loop_ms"] + t["checkpoint_ms"]) / t["iterations"]
+            best = per if best is None else min(best, per)
+        E.set_timing(0)
+        byt = iteration_bytes(m, n, nnz) + extra[name]
+        out[name] = {"us_per_iteration": round(best, 2), "algorithmic_bytes": byt,
+                     "algorithmic_gbs": round(byt / best / 1e3, 1), "frac_of_hbm": round(byt / best / 1e3 / peak, 3),
+                     "objective_after": r["objective"]}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -411,9 +453,12 @@ def main():
     ap.add_argument("--no-time-to-kkt", action="store_true")
     ap.add_argument("--batches", action="store_true", help="batched workloads instead of the headline line")
     ap.add_argument("--small", action="store_true", help="with --batches: 64 nodes and 256 LPs")
+    ap.add_argument("--qp", action="store_true", help="convex QP workload instead of the headline line")
     args = ap.parse_args()
     if args.batches:
         return run_batches(args)
+    if args.qp:
+        return run_qp(args)
     world, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
