@@ -187,20 +187,25 @@ def cpu_baseline(inst, target_seconds=12.0):
 
 def time_to_kkt(E, A, inst, eps=1e-6, limit_s=90.0):
     """Wall time of sankhya_b200_pdlp_solve to eps relative KKT on the same instance:
-    plain FP64 PDLP versus FP32 inner iterations with FP64 refinement (and an FP64
-    finish from the refined point). Host arrays in and out, scaling included."""
+    plain FP64 PDLP (GpuPdlp's restarted adaptive loop) versus FP32 inner iterations
+    with an FP64 finish, and the reflected restarted Halpern loop in FP64 and with the
+    FP32 phase. Host arrays in and out, scaling included."""
     out = {"eps": eps, "relative_kkt": "max(primal, dual, gap) as in GpuPdlp"}
-    for name, prec in (("fp64", E.FP64), ("fp32_refined", E.FP32_REFINE)):
+    runs = (("fp64", E.FP64, E.PDLP_ADAPTIVE), ("fp32_refined", E.FP32_REFINE, E.PDLP_ADAPTIVE),
+            ("halpern_fp64", E.FP64, E.PDLP_HALPERN), ("halpern_fp32_refined", E.FP32_REFINE, E.PDLP_HALPERN))
+    for name, prec, alg in runs:
         s = E.pdlp_default_settings()
         s.eps_optimal, s.precision, s.time_limit, s.max_iterations = eps, prec, limit_s, 2_000_000
+        s.algorithm = alg
         t0 = time.perf_counter()
         rc, x, y, r = E.pdlp_solve(A, inst, s)
         wall = time.perf_counter() - t0
         out[name] = {"seconds": round(wall, 3), "status": r["status"], "iterations": r["iterations"],
                      "refinements": r["refinements"], "objective": float(np.dot(inst["c"], x)),
                      "kkt": [r["relative_primal_residual"], r["relative_dual_residual"], r["relative_gap"]]}
-    if out["fp64"]["status"] == 0 and out["fp32_refined"]["status"] == 0:
-        out["speedup_mixed_vs_fp64"] = round(out["fp64"]["seconds"] / out["fp32_refined"]["seconds"], 3)
+    for name in ("fp32_refined", "halpern_fp64", "halpern_fp32_refined"):
+        if out["fp64"]["status"] == 0 and out[name]["status"] == 0:
+            out[f"speedup_{name}_vs_fp64"] = round(out["fp64"]["seconds"] / out[name]["seconds"], 3)
     return out
 
 
@@ -443,6 +448,38 @@ def run_qp(args):
     return 0
 
 
+def run_pdlp_compare(args):
+    """Restarted PDLP to 1e-6 relative KKT, GpuPdlp's adaptive loop versus the
+    reflected restarted Halpern loop (FP64, default scaling), on four seeded
+    instances of the engine's recipes. Prints one JSON line."""
+    E = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
+    I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    cases = (("lp_uniform(3, 20000, 40000, 5)", lambda: I.lp_uniform(3, 20000, 40000, 5)),
+             ("lp_powerlaw(5, 200000, 400000, 4000000)", lambda: I.lp_powerlaw(5, 200000, 400000, 4000000)),
+             ("milp_nodes(3, 1)[0]", lambda: I.milp_nodes(3, 1)[0]),
+             ("lp_family_base(4, 50000, 100000, 10)", lambda: I.lp_family_base(4, 50000, 100000, 10)))
+    rows = []
+    for name, make in cases:
+        inst = make()
+        A = E.Matrix.from_instance(inst)
+        row = {"instance": name}
+        for label, alg in (("adaptive", E.PDLP_ADAPTIVE), ("halpern", E.PDLP_HALPERN)):
+            s = E.pdlp_default_settings()
+            s.eps_optimal, s.time_limit, s.algorithm = 1e-6, 120.0, alg
+            E.pdlp_solve(A, inst, s)                     # warm-up: graphs, allocations
+            t = time.perf_counter()
+            rc, x, y, r = E.pdlp_solve(A, inst, s)
+            row[label] = {"seconds": round(time.perf_counter() - t, 4), "status": r["status"],
+                          "iterations": r["iterations"], "restarts": r["restarts"],
+                          "objective": float(np.dot(inst["c"], x))}
+        if row["adaptive"]["status"] == 0 and row["halpern"]["status"] == 0:
+            row["speedup_halpern"] = round(row["adaptive"]["seconds"] / row["halpern"]["seconds"], 3)
+        rows.append(row)
+    print(json.dumps({"metric": "PDLP wall time to 1e-6 relative KKT", "unit": "s", "higher_is_better": False,
+                      "data": "synthetic", "dtype": "f64", "cases": rows}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -454,7 +491,10 @@ def main():
     ap.add_argument("--batches", action="store_true", help="batched workloads instead of the headline line")
     ap.add_argument("--small", action="store_true", help="with --batches: 64 nodes and 256 LPs")
     ap.add_argument("--qp", action="store_true", help="convex QP workload instead of the headline line")
+    ap.add_argument("--pdlp-compare", action="store_true", help="adaptive versus Halpern PDLP on four instances")
     args = ap.parse_args()
+    if args.pdlp_compare:
+        return run_pdlp_compare(args)
     if args.batches:
         return run_batches(args)
     if args.qp:

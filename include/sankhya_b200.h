@@ -137,8 +137,14 @@ enum {
     SANKHYA_B200_FP32_REFINE = 1 /* FP32 inner iterations, FP64 refinement residuals */
 };
 
+enum {
+    SANKHYA_B200_PDLP_ADAPTIVE = 0, /* GpuPdlp's restarted adaptive PDHG (src/cuda/GpuPdlp.cpp:252-534) */
+    SANKHYA_B200_PDLP_HALPERN = 1   /* reflected restarted Halpern PDHG, constant step (no counterpart
+                                       in the reference; the method of cuPDLP+, Lu and Yang 2025)      */
+};
+
 typedef struct SankhyaB200PdlpSettings {
-    int struct_version;   /* 1 */
+    int struct_version;   /* 2 (1: the struct without `algorithm`, read as ADAPTIVE) */
     int max_iterations;   /* total PDHG iterations (accepted + rejected)          */
     int restart_period;   /* iterations between evaluations (GpuPdlp: 64)         */
     int power_iterations; /* power iterations for ||A||_2 (GpuPdlp: 30)           */
@@ -151,6 +157,8 @@ typedef struct SankhyaB200PdlpSettings {
     double eta_min_factor;/* 1e-6 */
     double eta_max_factor;/* 1e4  */
     double ruiz_tolerance;/* 1e-2 */
+    int algorithm;        /* SANKHYA_B200_PDLP_ADAPTIVE or SANKHYA_B200_PDLP_HALPERN  (version 2) */
+    int reserved;
 } SankhyaB200PdlpSettings;
 
 SANKHYA_CUDA_API void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* settings);

@@ -132,3 +132,54 @@ def test_fp32_refined_agrees_with_fp64_on_power_law(engine, instances):
     assert rc64 == 0 and rc32 == 0 and r64["status"] == 0 and r32["status"] == 0, (r64, r32)
     o64, o32 = float(np.dot(inst["c"], x64)), float(np.dot(inst["c"], x32))
     assert abs(o64 - o32) <= 1e-4 * (1 + abs(o64))
+
+
+# ------------------------------------------------------- reflected Halpern PDHG option
+
+@pytest.mark.parametrize("case", range(len(HAND)))
+def test_halpern_hand_solved_lps(engine, instances, case):
+    spec, ok = HAND[case]
+    inst = instances.small_dense_lp(**spec)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, algorithm=engine.PDLP_HALPERN))
+    assert rc == 0 and r["status"] == 0, r
+    assert r["rejected_steps"] == 0
+    assert ok(x), (x, r)
+
+
+@pytest.mark.parametrize("name,seed,m,n,per_col", [("lp60", 12, 60, 150, 4), ("lp300", 11, 300, 700, 5)])
+def test_halpern_reaches_simplex_objective(engine, instances, golden_dir, name, seed, m, n, per_col):
+    ref = json.load(open(os.path.join(golden_dir, f"simplex_{name}.json")))
+    inst = instances.lp_uniform(seed, m, n, per_col)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, algorithm=engine.PDLP_HALPERN, eps_optimal=1e-8))
+    assert rc == 0 and r["status"] == 0, r
+    assert max(r["relative_primal_residual"], r["relative_dual_residual"], r["relative_gap"]) <= 1e-8
+    obj = float(np.dot(inst["c"], x))
+    assert abs(obj - ref["objective"]) <= 1e-6 * (1 + abs(ref["objective"])), (obj, ref)
+
+
+def test_halpern_agrees_with_adaptive_on_power_law(engine, instances):
+    inst = instances.lp_powerlaw(21, 4000, 8000, 80000)
+    A = engine.Matrix.from_instance(inst)
+    rc_a, xa, ya, ra = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-6, time_limit=60.0))
+    rc_h, xh, yh, rh = engine.pdlp_solve(A, inst, settings(engine, algorithm=engine.PDLP_HALPERN, eps_optimal=1e-6,
+                                                             time_limit=60.0))
+    assert rc_a == 0 and rc_h == 0 and ra["status"] == 0 and rh["status"] == 0, (ra, rh)
+    oa, oh = float(np.dot(inst["c"], xa)), float(np.dot(inst["c"], xh))
+    assert abs(oa - oh) <= 1e-4 * (1 + abs(oa))
+
+
+def test_settings_version_one_means_adaptive(engine, instances):
+    import ctypes as C
+    spec, ok = HAND[0]
+    inst = instances.small_dense_lp(**spec)
+    A = engine.Matrix.from_instance(inst)
+    s = settings(engine, scaling=0)
+    s.struct_version = 1
+    s.algorithm = 99                      # not part of a version-1 struct: ignored
+    rc, x, y, r = engine.pdlp_solve(A, inst, s)
+    assert rc == 0 and r["status"] == 0 and ok(x)
+    s.struct_version = 2
+    rc, *_ = engine.pdlp_solve(A, inst, s)
+    assert rc == -1 and "invalid" in engine.last_error()

@@ -114,7 +114,7 @@ class PdlpSettings(C.Structure):
                 ("power_iterations", C.c_int), ("adaptive_step", C.c_int), ("scaling", C.c_int),
                 ("ruiz_iterations", C.c_int), ("precision", C.c_int), ("eps_optimal", C.c_double),
                 ("time_limit", C.c_double), ("eta_min_factor", C.c_double), ("eta_max_factor", C.c_double),
-                ("ruiz_tolerance", C.c_double)]
+                ("ruiz_tolerance", C.c_double), ("algorithm", C.c_int), ("reserved", C.c_int)]
 
 
 class PdlpResult(C.Structure):
@@ -152,6 +152,7 @@ class GnnSettings(C.Structure):
 
 SCALE_RUIZ, SCALE_POCK_CHAMBOLLE, SCALE_POW2 = 1, 2, 4
 FP64, FP32_REFINE = 0, 1
+PDLP_ADAPTIVE, PDLP_HALPERN = 0, 1
 
 
 def _declare(L):

@@ -31,6 +31,8 @@
 // relative gap never reached the inner tolerance.)
 #include "engine.cuh"
 
+#include <cstddef>
+
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -60,6 +62,7 @@ struct PdlpState {
     double eta_bar, dx_sq, dy_sq, interaction;
     unsigned int ticket;   // last-block election for the probe combine
     unsigned int pad;
+    double halpern_k0;     // Halpern path: iterations since the anchor at the window's start
 };
 
 template <class T>
@@ -245,6 +248,123 @@ struct PrimalFixedEpi {
     }
     __device__ __forceinline__ void finish(Acc&, double*) const {}
 };
+
+// Reflected Halpern PDHG (primal first). T(x, y) = (x+, y+) with
+// x+ = proj(x - tau (c + A'y)), y+ = prox(y + sigma A (2 x+ - x)); one Halpern step
+// z <- lambda (2 T(z) - z) + (1 - lambda) z0, lambda = (k + 1) / (k + 2), k the
+// iterations since the anchor z0. 2 x+ - x is also the dual step's point, so the
+// primal epilogue writes it to x_bar and the anchored primal update in place.
+template <class T>
+__device__ __forceinline__ T halpern_lambda(const PdlpState* st, int q) {
+    const double k = st->halpern_k0 + static_cast<double>(q);
+    return static_cast<T>((k + 1.0) / (k + 2.0));
+}
+
+template <class T>
+struct PrimalHalpernEpi {
+    T* __restrict__ x;
+    T* __restrict__ x_bar;
+    const T* __restrict__ x0;
+    const T* __restrict__ c;
+    const T* __restrict__ cl;
+    const T* __restrict__ cu;
+    const PdlpState* __restrict__ st;
+    int q;
+    using Acc = NoAcc;
+    __device__ __forceinline__ void row(int j, T aty, Acc&) const {
+        const T tau = static_cast<T>(st->eta / st->omega);
+        const T xj = x[j];
+        const T xr = T(2) * clampf<T>(xj - tau * (c[j] + aty), cl[j], cu[j]) - xj;
+        const T lam = halpern_lambda<T>(st, q);
+        x_bar[j] = xr;
+        x[j] = lam * xr + (T(1) - lam) * x0[j];
+    }
+    __device__ __forceinline__ void finish(Acc&, double*) const {}
+};
+
+template <class T>
+struct DualHalpernEpi {
+    T* __restrict__ y;
+    const T* __restrict__ y0;
+    const T* __restrict__ rl;
+    const T* __restrict__ ru;
+    const PdlpState* __restrict__ st;
+    int q;
+    using Acc = NoAcc;
+    __device__ __forceinline__ void row(int i, T axb, Acc&) const {
+        const T sigma = static_cast<T>(st->eta * st->omega);
+        const T yi = y[i];
+        const T v = yi + sigma * axb;
+        const T yr = T(2) * (v - sigma * clampf<T>(v / sigma, rl[i], ru[i])) - yi;
+        const T lam = halpern_lambda<T>(st, q);
+        y[i] = lam * yr + (T(1) - lam) * y0[i];
+    }
+    __device__ __forceinline__ void finish(Acc&, double*) const {}
+};
+
+// One plain application of T at the window's end: x_t = x+ (and x_bar = 2 x+ - x
+// for the dual half), y_t = y+, with sums |x+ - x|^2, |x+ - x0|^2 (and the dual
+// counterparts) for the fixed-point residual and the primal weight.
+template <class T>
+struct PrimalTEpi {
+    const T* __restrict__ x;
+    T* __restrict__ x_bar;
+    T* __restrict__ x_t;
+    const T* __restrict__ x0;
+    const T* __restrict__ c;
+    const T* __restrict__ cl;
+    const T* __restrict__ cu;
+    const PdlpState* __restrict__ st;
+    double* __restrict__ partial;
+    using Acc = Slots<2, 3u>;
+    __device__ __forceinline__ void row(int j, T aty, Acc& acc) const {
+        const T tau = static_cast<T>(st->eta / st->omega);
+        const T xj = x[j];
+        const T xp = clampf<T>(xj - tau * (c[j] + aty), cl[j], cu[j]);
+        x_t[j] = xp;
+        x_bar[j] = T(2) * xp - xj;
+        const double d = static_cast<double>(xp) - static_cast<double>(xj);
+        const double e = static_cast<double>(xp) - static_cast<double>(x0[j]);
+        acc.add(0, d * d);
+        acc.add(1, e * e);
+    }
+    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
+};
+
+template <class T>
+struct DualTEpi {
+    const T* __restrict__ y;
+    T* __restrict__ y_t;
+    const T* __restrict__ y0;
+    const T* __restrict__ rl;
+    const T* __restrict__ ru;
+    const PdlpState* __restrict__ st;
+    double* __restrict__ partial;
+    using Acc = Slots<2, 3u>;
+    __device__ __forceinline__ void row(int i, T axb, Acc& acc) const {
+        const T sigma = static_cast<T>(st->eta * st->omega);
+        const T yi = y[i];
+        const T v = yi + sigma * axb;
+        const T yp = v - sigma * clampf<T>(v / sigma, rl[i], ru[i]);
+        y_t[i] = yp;
+        const double d = static_cast<double>(yp) - static_cast<double>(yi);
+        const double e = static_cast<double>(yp) - static_cast<double>(y0[i]);
+        acc.add(0, d * d);
+        acc.add(1, e * e);
+    }
+    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
+};
+
+__global__ void k_set_halpern(PdlpState* st, double k0) { st->halpern_k0 = k0; }
+
+// Restart of the Halpern path: the new anchor and iterate are T(z).
+template <class T>
+__global__ void k_halpern_restart(int n, int m, const T* __restrict__ x_t, const T* __restrict__ y_t,
+                                  T* __restrict__ x, T* __restrict__ x0, T* __restrict__ y, T* __restrict__ y0) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) x[j] = x0[j] = x_t[j];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y[i] = y0[i] = y_t[i];
+}
 
 // ----------------------------------------------------------- residual kernels
 // PdlpKernels.cu:101-209 split over the two products, accumulated in FP64.
@@ -777,6 +897,7 @@ struct LoopParams {
     double cost_norm = 0.0, bound_norm = 0.0;
     double omega0 = 0.0;  // > 0: initial primal weight (else ||c|| / ||b||)
     double eta0 = 0.0;    // > 0: initial step size (else 0.9 / ||A||_2)
+    bool halpern = false; // reflected restarted Halpern PDHG instead of GpuPdlp's loop
 };
 
 struct LoopStats {
@@ -802,6 +923,7 @@ struct Core {
     PdlpState* st;
     double* host = nullptr;
     int grid_k2 = 1, grid_k3 = 1, grid_rr = 1, grid_rc = 1, grid_df = 1, grid_pf = 1;
+    int grid_ph = 1, grid_dh = 1, grid_pt = 1, grid_dt = 1;
     int launches = 0;
     std::vector<cudaGraphExec_t> graphs;
     Core() = default;
@@ -849,6 +971,10 @@ struct Core {
         grid_rc = tiled_grid<ResColsEpi<T>, T>(AT);
         grid_df = tiled_grid<DualFixedEpi<T>, T>(A);
         grid_pf = tiled_grid<PrimalFixedEpi<T>, T>(AT);
+        grid_ph = tiled_grid<PrimalHalpernEpi<T>, T>(AT);
+        grid_dh = tiled_grid<DualHalpernEpi<T>, T>(A);
+        grid_pt = tiled_grid<PrimalTEpi<T>, T>(AT);
+        grid_dt = tiled_grid<DualTEpi<T>, T>(A);
         for (auto g : graphs)
             if (g) cudaGraphExecDestroy(g);
         graphs.clear();
@@ -916,9 +1042,133 @@ struct Core {
         return 0;
     }
 
+    // One Halpern window: `period` anchored steps, then T at the window's end
+    // (into x_cand / y_cand), its residual sums (res[32..35]) and the relative KKT of
+    // T(z) (res[0..13]); x_restart / y_restart hold the anchor. A graph per (period,
+    // tau, sigma); the anchor offset comes from the device state.
+    int halpern_window(int period, int* graph_slot) {
+        cudaGraphExec_t exec = nullptr;
+        if (*graph_slot >= 0) exec = graphs[static_cast<size_t>(*graph_slot)];
+        if (!exec) {
+            const int saved = launches;
+            cudaGraph_t g;
+            B200_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            for (int q = 0; q < period; ++q) {
+                launch_tiled(AT, y, PrimalHalpernEpi<T>{x, x_bar, x_restart, c, cl, cu, st, q}, stream, grid_ph);
+                launch_tiled(A, x_bar, DualHalpernEpi<T>{y, y_restart, rl, ru, st, q}, stream, grid_dh);
+            }
+            launch_tiled(AT, y, PrimalTEpi<T>{x, x_bar, x_cand, x_restart, c, cl, cu, st, part_c}, stream, grid_pt);
+            k_combine<2, 3u><<<1, kThreads, 0, stream>>>(part_c, AT.ntiles ? grid_pt : 0, res + 32);
+            launch_tiled(A, x_bar, DualTEpi<T>{y, y_cand, y_restart, rl, ru, st, part_d}, stream, grid_dt);
+            k_combine<2, 3u><<<1, kThreads, 0, stream>>>(part_d, A.ntiles ? grid_dt : 0, res + 34);
+            residuals(x_cand, y_cand, nullptr, nullptr, res, 0);
+            cudaMemcpyAsync(host, res, 40 * sizeof(double), cudaMemcpyDeviceToHost, stream);
+            B200_TRY(cudaStreamEndCapture(stream, &g), "end capture");
+            cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail_cuda("graph instantiate", e);
+            if (*graph_slot >= 0) {
+                graphs[static_cast<size_t>(*graph_slot)] = exec;
+            } else {
+                graphs.push_back(exec);
+                *graph_slot = static_cast<int>(graphs.size()) - 1;
+            }
+            launches = saved;
+        }
+        B200_TRY(cudaGraphLaunch(exec, stream), "graph launch");
+        launches += 2 * period + 7;
+        return 0;
+    }
+
+    // Reflected restarted Halpern PDHG (the method of cuPDLP+, Lu and Yang 2025,
+    // restated): constant step eta = 0.9 / ||A||_2 split by the primal weight,
+    // restarts to T(z) when the fixed-point residual r = sqrt(omega |dx|^2 +
+    // |dy|^2 / omega) falls to 0.2 of its value at the last restart, or to 0.8
+    // and rises again, or after 0.36 of all iterations; at a restart the primal
+    // weight moves halfway (in log) to |y+ - y0| / |x+ - x0|. Termination on the
+    // relative KKT of T(z) at each window's end.
+    int run_halpern(const LoopParams& lp, LoopStats* out, const Plan* plan) {
+        const size_t nb = sizeof(T) * static_cast<size_t>(std::max(n, 1));
+        const size_t mb = sizeof(T) * static_cast<size_t>(std::max(m, 1));
+        for (T* v : {x_sum, x_cand, x_avg, aty}) cudaMemsetAsync(v, 0, nb, stream);
+        for (T* v : {y_sum, y_cand, y_avg, ax_cand, ax_avg}) cudaMemsetAsync(v, 0, mb, stream);
+        B200_TRY(cudaMemcpyAsync(x_restart, x, nb, cudaMemcpyDeviceToDevice, stream), "copy");
+        B200_TRY(cudaMemcpyAsync(y_restart, y, mb, cudaMemcpyDeviceToDevice, stream), "copy");
+        const double eta = kStepSafety / lp.matrix_norm;
+        double omega = 1.0;
+        if (lp.cost_norm > 0.0 && lp.bound_norm > 0.0)
+            omega = std::min(kMaxWeight, std::max(kMinWeight, lp.cost_norm / lp.bound_norm));
+        if (lp.omega0 > 0.0) omega = lp.omega0;
+        k_init_state<<<1, 1, 0, stream>>>(st, eta, omega, eta, eta);
+        B200_TRY(cudaGetLastError(), "Halpern setup");
+        long long iteration = 0, since_restart = 0;
+        double r_restart = std::numeric_limits<double>::infinity(), r_previous = r_restart;
+        int slot_full = -1, slot_tail = -1;
+        while (iteration < lp.max_iterations) {
+            const int period = static_cast<int>(std::min<long long>(lp.restart_period, lp.max_iterations - iteration));
+            if (period <= 0) break;
+            int* slot = period == lp.restart_period ? &slot_full : &slot_tail;
+            k_set_omega<<<1, 1, 0, stream>>>(st, omega, 0.0);
+            k_set_halpern<<<1, 1, 0, stream>>>(st, static_cast<double>(since_restart));
+            if (halpern_window(period, slot)) return -1;
+            B200_TRY(cudaStreamSynchronize(stream), "Halpern window");
+            ++out->syncs;
+            if (plan && plan->d_err) {
+                unsigned int word = 0;
+                if (cudaMemcpy(&word, plan->d_err, sizeof(word), cudaMemcpyDeviceToHost) == cudaSuccess && word) {
+                    cudaMemset(plan->d_err, 0, sizeof(word));
+                    return fail_msg("device wait gave up");
+                }
+            }
+            iteration += period;
+            since_restart += period;
+            const double* h = host;
+            const Kkt kkt = to_kkt(h, lp.cost_norm, lp.bound_norm);
+            out->best = kkt;
+            const double dx2 = h[32], dx0 = h[33], dy2 = h[34], dy0 = h[35];
+            if (!std::isfinite(kkt.primal) || !std::isfinite(dx2) || !std::isfinite(dy2)) {
+                out->numeric = true;
+                break;
+            }
+            if (kkt.primal <= lp.eps && kkt.dual <= lp.eps && kkt.gap <= lp.eps) {
+                B200_TRY(cudaMemcpyAsync(x, x_cand, nb, cudaMemcpyDeviceToDevice, stream), "copy");
+                B200_TRY(cudaMemcpyAsync(y, y_cand, mb, cudaMemcpyDeviceToDevice, stream), "copy");
+                out->converged = true;
+                break;
+            }
+            if (lp.deadline > 0.0 && now_s() > lp.deadline) {
+                out->timed_out = true;
+                break;
+            }
+            const double r = std::sqrt(omega * dx2 + dy2 / omega);
+            const bool sufficient = r <= kSufficient * r_restart;
+            const bool necessary = r <= kNecessary * r_restart && r > r_previous;
+            const bool artificial = static_cast<double>(since_restart) >= kArtificial * static_cast<double>(iteration);
+            r_previous = r;
+            if (!(sufficient || necessary || artificial)) continue;
+            k_halpern_restart<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, x_cand, y_cand, x, x_restart, y,
+                                                                               y_restart);
+            ++launches;
+            since_restart = 0;
+            r_restart = r;
+            r_previous = std::numeric_limits<double>::infinity();
+            ++out->restarts;
+            if (dx0 > 1e-28 && dy0 > 1e-28) {
+                const double target = std::sqrt(dy0 / dx0);
+                const double updated = std::exp(kSmoothing * std::log(target) + (1.0 - kSmoothing) * std::log(omega));
+                if (std::isfinite(updated)) omega = std::min(kMaxWeight, std::max(kMinWeight, updated));
+            }
+        }
+        out->iterations += iteration;
+        out->omega = omega;
+        out->eta = eta;
+        return 0;
+    }
+
     // Starting point already in x, y (T). Sets up A x, the restart reference
     // and the step state, then runs restarted windows (GpuPdlp.cpp:252-534).
     int run(const LoopParams& lp, LoopStats* out, const Plan* plan) {
+        if (lp.halpern) return run_halpern(lp, out, plan);
         const size_t nb = sizeof(T) * static_cast<size_t>(std::max(n, 1));
         const size_t mb = sizeof(T) * static_cast<size_t>(std::max(m, 1));
         for (T* v : {x_sum, x_cand, x_avg, aty}) cudaMemsetAsync(v, 0, nb, stream);
@@ -1039,7 +1289,7 @@ using namespace b200;
 extern "C" void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* s) {
     if (!s) return;
     std::memset(s, 0, sizeof(*s));
-    s->struct_version = 1;
+    s->struct_version = 2;
     s->max_iterations = 500000;
     s->restart_period = 64;
     s->power_iterations = 30;
@@ -1066,9 +1316,18 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     SankhyaB200PdlpSettings s;
     sankhya_b200_pdlp_default_settings(&s);
     if (settings) {
-        if (settings->struct_version != 1) return fail_msg("unsupported settings struct_version");
-        s = *settings;
+        if (settings->struct_version == 1) {
+            std::memcpy(&s, settings, offsetof(SankhyaB200PdlpSettings, algorithm));
+            s.struct_version = 2;
+            s.algorithm = SANKHYA_B200_PDLP_ADAPTIVE;
+        } else if (settings->struct_version == 2) {
+            s = *settings;
+        } else {
+            return fail_msg("unsupported settings struct_version");
+        }
     }
+    if (s.algorithm != SANKHYA_B200_PDLP_ADAPTIVE && s.algorithm != SANKHYA_B200_PDLP_HALPERN)
+        return fail_msg("invalid PDLP settings");
     if (!matrix || !c || !row_lower || !row_upper || !col_lower || !col_upper || !x_out)
         return fail_msg("null model or output pointer");
     if (s.max_iterations <= 0 || s.restart_period <= 0 || s.power_iterations < 0 || !(s.eps_optimal > 0.0) ||
@@ -1119,6 +1378,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     LoopParams lp;
     lp.restart_period = s.restart_period;
     lp.adaptive = s.adaptive_step != 0;
+    lp.halpern = s.algorithm == SANKHYA_B200_PDLP_HALPERN;
     lp.deadline = s.time_limit > 0.0 ? t_start + s.time_limit : 0.0;
     lp.matrix_norm = matrix_norm;
     lp.eta_min_factor = s.eta_min_factor;
@@ -1222,7 +1482,8 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     result->status = stats.numeric ? -2 : stats.converged ? 0 : stats.timed_out ? 2 : 1;
     result->iterations = static_cast<int>(std::min<long long>(stats.iterations, 2147483647LL));
     result->restarts = stats.restarts;
-    result->rejected_steps = lp.adaptive ? static_cast<int>(std::max(0.0, stats.updates - stats.accept_count)) : 0;
+    result->rejected_steps = (lp.adaptive && !lp.halpern)
+                                 ? static_cast<int>(std::max(0.0, stats.updates - stats.accept_count)) : 0;
     result->host_syncs = syncs;
     result->refinements = refinements;
     result->primal_objective = best.pobj;
@@ -1231,7 +1492,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     result->relative_dual_residual = best.dual;
     result->relative_gap = best.gap;
     result->matrix_norm = matrix_norm;
-    result->final_step_size = lp.adaptive ? stats.eta : kStepSafety / matrix_norm;
+    result->final_step_size = (lp.adaptive && !lp.halpern) ? stats.eta : kStepSafety / matrix_norm;
     result->primal_weight = stats.omega;
     result->seconds = now_s() - t_start;
     ts.last.iterations = result->iterations;
