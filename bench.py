@@ -381,6 +381,12 @@ def run_batches(args):
     bp = (nodes_n + 31) // 32 * 32
     shared_bytes = (2 * 12 * nnz + 4 * (m + 1) + 4 * (n + 1) + 8 * bp * (n + 2 * m) + 8 * bp * (m + 5 * n)
                     + 16 * (m + n))
+    if args.nodes_only:
+        print(json.dumps({"metric": "batched PDHG, device time per iteration (CUDA events around the iteration loop)",
+                          "unit": "us", "higher_is_better": False, "data": "synthetic", "dtype": "f64",
+                          "node_relaxations": {"workload": f"{nodes_n} node relaxations sharing A",
+                                               "shared_matrix_us": round(shared, 2)}}))
+        return 0
     blk, rseg, cseg = E.block_diagonal(nodes)
     B = E.Matrix.from_instance(blk)
     blockdiag = _device_us(E, lambda s: E.batch_pdhg(B, blk, rseg, cseg, s)[0], settings, 2000)
@@ -490,6 +496,7 @@ def main():
     ap.add_argument("--no-time-to-kkt", action="store_true")
     ap.add_argument("--batches", action="store_true", help="batched workloads instead of the headline line")
     ap.add_argument("--small", action="store_true", help="with --batches: 64 nodes and 256 LPs")
+    ap.add_argument("--nodes-only", action="store_true", help="with --batches: the shared-matrix node batch only")
     ap.add_argument("--qp", action="store_true", help="convex QP workload instead of the headline line")
     ap.add_argument("--pdlp-compare", action="store_true", help="adaptive versus Halpern PDLP on four instances")
     args = ap.parse_args()
