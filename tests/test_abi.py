@@ -46,3 +46,37 @@ def test_no_device_is_a_clean_error(engine):
         return
     rc, y = engine.spmv_host(2, 3, [0, 2, 4], [0, 2, 1, 2], [1.0, 2, 3, 4], [2.0, 5, 7])
     assert rc != 0 and "device" in engine.last_error().lower()
+
+
+def test_every_solver_entry_fails_without_a_device(engine, instances):
+    """No host path behind any solver entry point: without a GPU each returns -1 with
+    an error text (checked where this suite runs without one)."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    if torch.cuda.is_available():
+        return
+    L = engine.lib()
+    inst = instances.lp_uniform(1, 8, 12, 2)
+    csr = engine.CSR()
+    p = lambda a, t=C.c_int: np.ascontiguousarray(a, dtype=np.int32 if t is C.c_int else np.float64).ctypes.data_as(
+        C.POINTER(t))
+    rc = L.sankhya_cuda_csr_create(C.byref(csr), inst["m"], inst["n"], int(inst["ptr"][-1]), p(inst["ptr"]),
+                                   p(inst["idx"]), p(inst["val"], C.c_double))
+    assert rc != 0 and "device" in engine.last_error().lower()
+    net = C.c_void_p()
+    assert L.sankhya_b200_gnn_create(None, C.byref(net)) == -1 and not net.value
+    assert "device" in engine.last_error().lower()
+    s = engine.batch_default_settings()
+    x = np.zeros(2 * inst["n"])
+    res = (engine.BatchResult * 2)()
+    d = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double))
+    fake = engine.CSR(inst["m"], inst["n"], int(inst["ptr"][-1]), None, None, None)
+    rc = L.sankhya_b200_shared_batch_pdhg(C.byref(fake), 2, d(inst["c"]), 0, d(inst["rl"]), d(inst["ru"]), 0,
+                                          d(inst["cl"]), d(inst["cu"]), 0, C.byref(s), d(x), None, res)
+    assert rc == -1 and "device" in engine.last_error().lower()
+    ps = engine.pdlp_default_settings()
+    pr = engine.PdlpResult()
+    rc = L.sankhya_b200_pdlp_solve(C.byref(fake), d(inst["c"]), d(inst["rl"]), d(inst["ru"]), d(inst["cl"]),
+                                   d(inst["cu"]), C.byref(ps), None, None, d(x), None, C.byref(pr))
+    assert rc == -1 and "device" in engine.last_error().lower()
