@@ -144,7 +144,7 @@ enum {
 };
 
 typedef struct SankhyaB200PdlpSettings {
-    int struct_version;   /* 2 (1: the struct without `algorithm`, read as ADAPTIVE) */
+    int struct_version;   /* 3 (2: without initial_primal_weight; 1: also without algorithm) */
     int max_iterations;   /* total PDHG iterations (accepted + rejected)          */
     int restart_period;   /* iterations between evaluations (GpuPdlp: 64)         */
     int power_iterations; /* power iterations for ||A||_2 (GpuPdlp: 30)           */
@@ -159,6 +159,8 @@ typedef struct SankhyaB200PdlpSettings {
     double ruiz_tolerance;/* 1e-2 */
     int algorithm;        /* SANKHYA_B200_PDLP_ADAPTIVE or SANKHYA_B200_PDLP_HALPERN  (version 2) */
     int reserved;
+    double initial_primal_weight; /* > 0: start from this primal weight (e.g. one learned
+                                     for an LP family); 0: ||c|| / ||b|| (version 3)      */
 } SankhyaB200PdlpSettings;
 
 SANKHYA_CUDA_API void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* settings);

@@ -71,16 +71,33 @@ def test_prediction_inside_bounds(engine, instances):
     assert np.all(x >= lo) and np.all(x <= hi)
 
 
-def test_trained_network_warm_start_beats_cold_start(engine, instances, learned):
+def test_what_training_gains_on_held_out_members(engine, instances, learned):
+    """Trained on 64 solved members of a family, measured on 64 others: the held-out
+    loss falls far below the untrained network's, the predictions are closer to the
+    solutions than the training mean is (the trivial predictor), every warm-started
+    PDLP solve converges (PDLP's own KKT test judges it), and the warm starts need
+    fewer iterations on average than cold starts."""
     base = instances.lp_family_base(11, 150, 375, 4)
     A = engine.Matrix.from_instance(base)
     train = learned.dataset(engine, A, [instances.lp_family_member(base, 1000 + s) for s in range(64)], 1e-6)
-    assert len(train) == 64
-    net = engine.Gnn(seed=3, y_scale=learned.dual_scale(train))
+    held = learned.dataset(engine, A, [instances.lp_family_member(base, 5000 + s) for s in range(64)], 1e-6)
+    assert len(train) == 64 and len(held) == 64
+    scale = learned.dual_scale(train)
+    net, untrained = engine.Gnn(seed=3, y_scale=scale), engine.Gnn(seed=3, y_scale=scale)
     history = learned.train(net, A, train, 40)
     assert history[-1] < 0.25 * history[0]
-    rows = learned.evaluate(engine, net, A, [instances.lp_family_member(base, 5000 + s) for s in range(16)], 1e-6)
+    loss = lambda g: np.mean([g.gradient(A, d[0], d[1], d[2])[0] for d in held])
+    assert loss(net) < 0.2 * loss(untrained)
+    mx, my = np.mean([d[1] for d in train], axis=0), np.mean([d[2] for d in train], axis=0)
+
+    def err(xp, yp, d):
+        return np.sqrt(np.mean((xp - d[1]) ** 2)), np.sqrt(np.mean((yp - d[2]) ** 2))
+
+    e_net = np.mean([err(*net.predict(A, d[0]), d) for d in held], axis=0)
+    e_mean = np.mean([err(mx, my, d) for d in held], axis=0)
+    assert e_net[0] < e_mean[0] and e_net[1] < e_mean[1], (e_net, e_mean)
+    rows = learned.evaluate(engine, net, A, [d[0] for d in held], 1e-6)
     assert all(r["cold_status"] == 0 and r["warm_status"] == 0 for r in rows)
     cold = np.mean([r["cold_iterations"] for r in rows])
     warm = np.mean([r["warm_iterations"] for r in rows])
-    assert warm <= 0.95 * cold, (warm, cold)
+    assert warm <= 0.97 * cold, (warm, cold)

@@ -114,7 +114,8 @@ class PdlpSettings(C.Structure):
                 ("power_iterations", C.c_int), ("adaptive_step", C.c_int), ("scaling", C.c_int),
                 ("ruiz_iterations", C.c_int), ("precision", C.c_int), ("eps_optimal", C.c_double),
                 ("time_limit", C.c_double), ("eta_min_factor", C.c_double), ("eta_max_factor", C.c_double),
-                ("ruiz_tolerance", C.c_double), ("algorithm", C.c_int), ("reserved", C.c_int)]
+                ("ruiz_tolerance", C.c_double), ("algorithm", C.c_int), ("reserved", C.c_int),
+                ("initial_primal_weight", C.c_double)]
 
 
 class PdlpResult(C.Structure):

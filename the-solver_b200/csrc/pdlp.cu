@@ -1289,7 +1289,7 @@ using namespace b200;
 extern "C" void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* s) {
     if (!s) return;
     std::memset(s, 0, sizeof(*s));
-    s->struct_version = 2;
+    s->struct_version = 3;
     s->max_iterations = 500000;
     s->restart_period = 64;
     s->power_iterations = 30;
@@ -1318,15 +1318,18 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     if (settings) {
         if (settings->struct_version == 1) {
             std::memcpy(&s, settings, offsetof(SankhyaB200PdlpSettings, algorithm));
-            s.struct_version = 2;
-            s.algorithm = SANKHYA_B200_PDLP_ADAPTIVE;
         } else if (settings->struct_version == 2) {
+            std::memcpy(&s, settings, offsetof(SankhyaB200PdlpSettings, initial_primal_weight));
+        } else if (settings->struct_version == 3) {
             s = *settings;
         } else {
             return fail_msg("unsupported settings struct_version");
         }
     }
+    s.struct_version = 3;
     if (s.algorithm != SANKHYA_B200_PDLP_ADAPTIVE && s.algorithm != SANKHYA_B200_PDLP_HALPERN)
+        return fail_msg("invalid PDLP settings");
+    if (!(s.initial_primal_weight >= 0.0) || !std::isfinite(s.initial_primal_weight))
         return fail_msg("invalid PDLP settings");
     if (!matrix || !c || !row_lower || !row_upper || !col_lower || !col_upper || !x_out)
         return fail_msg("null model or output pointer");
@@ -1379,6 +1382,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     lp.restart_period = s.restart_period;
     lp.adaptive = s.adaptive_step != 0;
     lp.halpern = s.algorithm == SANKHYA_B200_PDLP_HALPERN;
+    if (s.initial_primal_weight > 0.0) lp.omega0 = std::min(kMaxWeight, std::max(kMinWeight, s.initial_primal_weight));
     lp.deadline = s.time_limit > 0.0 ? t_start + s.time_limit : 0.0;
     lp.matrix_norm = matrix_norm;
     lp.eta_min_factor = s.eta_min_factor;

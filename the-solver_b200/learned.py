@@ -15,22 +15,24 @@ import time
 import numpy as np
 
 
-def solve(engine, matrix, inst, eps, x0=None, y0=None, max_iterations=200_000):
+def solve(engine, matrix, inst, eps, x0=None, y0=None, max_iterations=200_000, omega0=None):
     s = engine.pdlp_default_settings()
     s.eps_optimal = eps
     s.max_iterations = max_iterations
+    if omega0:
+        s.initial_primal_weight = omega0
     t = time.perf_counter()
     rc, x, y, res = engine.pdlp_solve(matrix, inst, s, x0=x0, y0=y0)
     return rc, x, y, res, time.perf_counter() - t
 
 
 def dataset(engine, matrix, members, eps, progress=None):
-    """(member, x*, y*) for every member whose PDLP solve converged."""
+    """(member, x*, y*, final primal weight) for every member whose PDLP solve converged."""
     out = []
     for k, inst in enumerate(members):
         rc, x, y, res, _ = solve(engine, matrix, inst, eps)
         if rc == 0 and res["status"] == 0:
-            out.append((inst, x, y))
+            out.append((inst, x, y, res["primal_weight"]))
         if progress and (k + 1) % progress == 0:
             import sys
             print(f"solved {k + 1} / {len(members)}", file=sys.stderr, flush=True)
@@ -39,7 +41,7 @@ def dataset(engine, matrix, members, eps, progress=None):
 
 def dual_scale(data):
     """Scale of the dual targets: their root mean square (at least 1e-12)."""
-    ys = np.concatenate([y for _, _, y in data])
+    ys = np.concatenate([d[2] for d in data])
     return float(max(np.sqrt(np.mean(ys ** 2)), 1e-12))
 
 
@@ -53,10 +55,18 @@ def train(gnn, matrix, data, epochs, seed=0):
     return history
 
 
-def evaluate(engine, gnn, matrix, members, eps, mean_x=None, mean_y=None):
+def learned_weight(data):
+    """The family's primal weight: the median of the training solves' final weights."""
+    return float(np.median([d[3] for d in data]))
+
+
+def evaluate(engine, gnn, matrix, members, eps, mean_x=None, mean_y=None, omega=None):
     """Per member: cold-start and network-warm-started PDLP (and, given the
-    training mean, a mean-solution warm start): iterations, seconds, status."""
+    training mean, a mean-solution warm start; given a learned primal weight, both
+    starts again from that weight): iterations, seconds, status."""
     rows = []
+    if members:  # one untimed solve first: graph capture and allocations are not a start's cost
+        solve(engine, matrix, members[0], eps)
     for inst in members:
         rc_c, _, _, cold, t_cold = solve(engine, matrix, inst, eps)
         tp = time.perf_counter()
@@ -70,6 +80,12 @@ def evaluate(engine, gnn, matrix, members, eps, mean_x=None, mean_y=None):
         if mean_x is not None:
             _, _, _, mean, t_mean = solve(engine, matrix, inst, eps, x0=mean_x, y0=mean_y)
             row.update(mean_iterations=mean["iterations"], mean_seconds=t_mean, mean_status=mean["status"])
+        if omega:
+            _, _, _, cw, t_cw = solve(engine, matrix, inst, eps, omega0=omega)
+            _, _, _, ww, t_ww = solve(engine, matrix, inst, eps, x0=xp, y0=yp, omega0=omega)
+            row.update(cold_weight_iterations=cw["iterations"], cold_weight_seconds=t_cw,
+                       cold_weight_status=cw["status"], warm_weight_iterations=ww["iterations"],
+                       warm_weight_seconds=t_ww + t_pred, warm_weight_status=ww["status"])
         rows.append(row)
     return rows
 
@@ -135,8 +151,9 @@ def main(argv=None):
     t_train = time.perf_counter() - t
     mean_x = np.mean([d[1] for d in data], axis=0)
     mean_y = np.mean([d[2] for d in data], axis=0)
+    omega = learned_weight(data)
     rows = evaluate(engine, net, matrix, [instances.lp_family_member(base, 900_000 + s) for s in range(a.eval)], a.eps,
-                    mean_x, mean_y)
+                    mean_x, mean_y, omega)
     avg = lambda k: float(np.mean([r[k] for r in rows])) if rows else None
     out = dict(workload=f"lp_family: m={a.m}, n={a.n}, {a.per_col} per column, seed {a.seed}",
                nnz=int(base["ptr"][-1]), eps=a.eps, train_members=len(data), train_eps=a.train_eps,
@@ -148,8 +165,13 @@ def main(argv=None):
                cold_iterations=avg("cold_iterations"), warm_iterations=avg("warm_iterations"),
                mean_start_iterations=avg("mean_iterations"), cold_seconds=avg("cold_seconds"),
                warm_seconds=avg("warm_seconds"), predict_seconds=avg("predict_seconds"),
-               mean_start_seconds=avg("mean_seconds"))
+               mean_start_seconds=avg("mean_seconds"), learned_primal_weight=omega,
+               cold_weight_iterations=avg("cold_weight_iterations"), cold_weight_seconds=avg("cold_weight_seconds"),
+               warm_weight_iterations=avg("warm_weight_iterations"), warm_weight_seconds=avg("warm_weight_seconds"),
+               converged_warm_weight=sum(r["warm_weight_status"] == 0 for r in rows))
     out["speedup_warm_vs_cold"] = out["cold_seconds"] / out["warm_seconds"] if rows else None
+    out["speedup_weight_vs_cold"] = out["cold_seconds"] / out["cold_weight_seconds"] if rows else None
+    out["speedup_warm_weight_vs_cold"] = out["cold_seconds"] / out["warm_weight_seconds"] if rows else None
     print(json.dumps(out))
 
 
