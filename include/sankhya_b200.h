@@ -261,7 +261,7 @@ SANKHYA_CUDA_API int sankhya_b200_shared_batch_pdhg(
    varying cost and bounds). No counterpart in the reference, which has no
    learned component and always starts PDLP from zero (src/cuda/GpuPdlp.cpp:278-290);
    the prediction goes to sankhya_b200_pdlp_solve as x0 / y0, cold start stays
-   the fallback, and PDLP's own relative-KKT test judges every answer.
+   the fallback, and PDLP's own relative-KKT test decides every answer.
    Network: 16 node features, 4 rounds (settable) of width 64, bf16 tensor-core
    dense layers with fp32 accumulation, fp32 aggregation; trained with Adam on
    (instance, solution) pairs, one instance per step. Deterministic. */

@@ -75,7 +75,7 @@ def test_what_training_gains_on_held_out_members(engine, instances, learned):
     """Trained on 64 solved members of a family, measured on 64 others: the held-out
     loss falls far below the untrained network's, the predictions are closer to the
     solutions than the training mean is (the trivial predictor), every warm-started
-    PDLP solve converges (PDLP's own KKT test judges it), and the warm starts need
+    PDLP solve converges (PDLP's own KKT test decides it), and the warm starts need
     fewer iterations on average than cold starts."""
     base = instances.lp_family_base(11, 150, 375, 4)
     A = engine.Matrix.from_instance(base)

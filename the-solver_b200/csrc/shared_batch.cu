@@ -36,8 +36,9 @@ constexpr int kSlabs = 2;                 // 32-LP slabs carried by one warp
 constexpr int kGroupLps = 32 * kSlabs;    // LPs per warp unit
 constexpr int kAhead = 4;                 // row entries whose gathers are issued together
 
-// Each epilogue loads its per-(row, LP) data before the gathers (load) and
-// finishes the step with the row sum (store).
+// Each epilogue prefetches its per-(row, LP) data into L1 before the gathers
+// (prefetch: no registers held), reads it after them (load) and finishes the step
+// with the row sum (store).
 
 // sk_solve.c:901-906 per (row, LP), with LP freezing
 struct MultiDualEpi {
@@ -55,6 +56,12 @@ struct MultiDualEpi {
     __device__ __forceinline__ Row load(int i, int k) const {
         const size_t e = static_cast<size_t>(i) * bp + k, b = rows_per_lp ? e : static_cast<size_t>(i);
         return Row{y[e], rl[b], ru[b], done[k]};
+    }
+    __device__ __forceinline__ void prefetch(int i, int k) const {
+        const size_t e = static_cast<size_t>(i) * bp + k, b = rows_per_lp ? e : static_cast<size_t>(i);
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(y + e));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(rl + b));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(ru + b));
     }
     __device__ __forceinline__ void store(int i, int k, double act, const Row& r) const {
         const size_t e = static_cast<size_t>(i) * bp + k;
@@ -87,6 +94,12 @@ struct MultiPrimalEpi {
         const size_t e = static_cast<size_t>(j) * bp + k;
         return Row{x[e], c[c_per_lp ? e : static_cast<size_t>(j)], cl[e], cu[e], done[k]};
     }
+    __device__ __forceinline__ void prefetch(int j, int k) const {
+        const size_t e = static_cast<size_t>(j) * bp + k;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(x + e));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(cl + e));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(cu + e));
+    }
     __device__ __forceinline__ void store(int j, int k, double g, const Row& r) const {
         const size_t e = static_cast<size_t>(j) * bp + k;
         if (r.frozen) {
@@ -105,6 +118,7 @@ struct MultiStoreEpi {
     int bp;
     struct Row {};
     __device__ __forceinline__ Row load(int, int) const { return {}; }
+    __device__ __forceinline__ void prefetch(int, int) const {}
     __device__ __forceinline__ void store(int i, int k, double s, const Row&) const {
         out[static_cast<size_t>(i) * bp + k] = s;
     }
@@ -125,10 +139,9 @@ __global__ void __launch_bounds__(kThreads) k_multi(int rows, int groups, int bp
         const int r = static_cast<int>(u / groups), g = static_cast<int>(u % groups);
         const int k0 = g * kGroupLps;
         const int ns = min(kSlabs, (bp - k0) >> 5);
-        typename Epi::Row pre[kSlabs];
 #pragma unroll
         for (int s = 0; s < kSlabs; ++s)
-            if (s < ns) pre[s] = epi.load(r, k0 + 32 * s + lane);
+            if (s < ns) epi.prefetch(r, k0 + 32 * s + lane);
         double acc[kSlabs];
 #pragma unroll
         for (int s = 0; s < kSlabs; ++s) acc[s] = 0.0;
@@ -163,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) k_multi(int rows, int groups, int bp
         }
 #pragma unroll
         for (int s = 0; s < kSlabs; ++s)
-            if (s < ns) epi.store(r, k0 + 32 * s + lane, acc[s], pre[s]);
+            if (s < ns) epi.store(r, k0 + 32 * s + lane, acc[s], epi.load(r, k0 + 32 * s + lane));
     }
 }
 
