@@ -203,7 +203,10 @@ typedef struct SankhyaB200BatchSettings {
     int struct_version;  /* 1 */
     int max_iterations;  /* per LP (100000, sk_solve's default)              */
     int check_every;     /* 20, as in sk_solve                               */
-    int reserved;
+    int schedule;        /* shared-matrix batch only: 0 = warp shape picked by timing
+                            (cached per matrix and batch width), 1..3 = fixed shape
+                            (1 x 8, 2 x 4, 4 x 4 slabs x look-ahead); results do not
+                            depend on it                                      */
     double primal_tol;   /* 1e-7 */
     double dual_tol;     /* 1e-7 */
     double time_limit;   /* seconds for the whole batch, <= 0 for none        */

@@ -94,3 +94,21 @@ def test_rejects_crossed_bounds(engine, instances):
     nodes[1]["cl"][5] = 2.0                  # above the upper bound of 1
     rc, *_ = _shared(engine, nodes, _settings(engine, 100, 1e-6, 1e-6))
     assert rc == -1 and "bound" in engine.last_error()
+
+
+def test_every_warp_schedule_gives_the_same_bits(engine, instances):
+    # 70 LPs: 3 slabs, so each shape (1 x 8, 2 x 4, 4 x 4) has a partly filled group
+    nodes = instances.milp_nodes(40, 70, m=300, n=600)
+    outs = []
+    for schedule in (0, 1, 2, 3):
+        s = _settings(engine, 400, 1e-5, 1e-5)
+        s.schedule = schedule
+        rc, x, y, res = _shared(engine, nodes, s)
+        assert rc == 0, engine.last_error()
+        outs.append((x, y, res))
+    for x, y, res in outs[1:]:
+        assert np.array_equal(x, outs[0][0]) and np.array_equal(y, outs[0][1]) and res == outs[0][2]
+    s = _settings(engine, 10, 1e-5, 1e-5)
+    s.schedule = 4
+    rc, *_ = _shared(engine, nodes, s)
+    assert rc == -1 and "settings" in engine.last_error()

@@ -134,7 +134,7 @@ class PdlpResult(C.Structure):
 class BatchSettings(C.Structure):
     """SankhyaB200BatchSettings."""
     _fields_ = [("struct_version", C.c_int), ("max_iterations", C.c_int), ("check_every", C.c_int),
-                ("reserved", C.c_int), ("primal_tol", C.c_double), ("dual_tol", C.c_double),
+                ("schedule", C.c_int), ("primal_tol", C.c_double), ("dual_tol", C.c_double),
                 ("time_limit", C.c_double)]
 
 

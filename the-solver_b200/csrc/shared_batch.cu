@@ -8,7 +8,7 @@
 // Layout. The per-LP vectors live batch-minor on the device: element j of LP k
 // at j * bp + k, bp = batch rounded up to 32. A row of the shared matrix is read
 // once per iteration for all LPs; its "gathers" become contiguous 256-byte
-// loads of 32 LPs' values (one slab), and a warp carries kSlabs slabs through
+// loads of 32 LPs' values (one slab), and a warp carries a few slabs through
 // the row, one LP per lane and slab. Each LP's row sum runs over
 // the row's entries in stored order with unfused products and adds, the order
 // and rounding of sk_solve's serial CSC loops (and of the single-LP kernels'
@@ -19,6 +19,8 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace b200 {
@@ -32,9 +34,14 @@ using batch::sk_inf;
 using batch::sk_neg_inf;
 using batch::slot_value;
 
-constexpr int kSlabs = 2;                 // 32-LP slabs carried by one warp
-constexpr int kGroupLps = 32 * kSlabs;    // LPs per warp unit
-constexpr int kAhead = 4;                 // row entries whose gathers are issued together
+// Warp shapes: S 32-LP slabs carried by one warp, gathers of A row entries issued
+// together. Every shape sums each LP in stored order, so all give the same bits;
+// the fastest for a (matrix, batch width) is picked by timing (schedule 0) or
+// fixed by the caller (schedule 1..3).
+struct Shape {
+    int slabs, ahead;
+};
+constexpr Shape kShapes[3] = {{1, 8}, {2, 4}, {4, 4}};
 
 // Each epilogue prefetches its per-(row, LP) data into L1 before the gathers
 // (prefetch: no registers held), reads it after them (load) and finishes the step
@@ -124,10 +131,10 @@ struct MultiStoreEpi {
     }
 };
 
-// One warp per (row, group of kGroupLps LPs): out(r, k) = sum_p a_p v[col_p, k]
-// in stored order for every LP k of the group. The gathers of kAhead entries are
-// issued before their products are added, in order, to each LP's sum.
-template <class Epi>
+// One warp per (row, group of 32 S LPs): out(r, k) = sum_p a_p v[col_p, k] in
+// stored order for every LP k of the group. The gathers of AH entries are issued
+// before their products are added, in order, to each LP's sum.
+template <class Epi, int S, int AH>
 __global__ void __launch_bounds__(kThreads) k_multi(int rows, int groups, int bp, const int* __restrict__ ptr,
                                                     const int* __restrict__ idx, const double* __restrict__ val,
                                                     const double* __restrict__ v, Epi epi) {
@@ -137,14 +144,14 @@ __global__ void __launch_bounds__(kThreads) k_multi(int rows, int groups, int bp
     const long long nw = static_cast<long long>(gridDim.x) * kWarps;
     for (long long u = static_cast<long long>(blockIdx.x) * kWarps + (threadIdx.x >> 5); u < units; u += nw) {
         const int r = static_cast<int>(u / groups), g = static_cast<int>(u % groups);
-        const int k0 = g * kGroupLps;
-        const int ns = min(kSlabs, (bp - k0) >> 5);
+        const int k0 = g * 32 * S;
+        const int ns = min(S, (bp - k0) >> 5);
 #pragma unroll
-        for (int s = 0; s < kSlabs; ++s)
+        for (int s = 0; s < S; ++s)
             if (s < ns) epi.prefetch(r, k0 + 32 * s + lane);
-        double acc[kSlabs];
+        double acc[S];
 #pragma unroll
-        for (int s = 0; s < kSlabs; ++s) acc[s] = 0.0;
+        for (int s = 0; s < S; ++s) acc[s] = 0.0;
         const int p0 = __ldg(ptr + r), p1 = __ldg(ptr + r + 1);
         for (int pb = p0; pb < p1; pb += 32) {
             const int cnt = min(32, p1 - pb);
@@ -154,28 +161,28 @@ __global__ void __launch_bounds__(kThreads) k_multi(int rows, int groups, int bp
                 ci = __ldg(idx + pb + lane);
                 ai = __ldg(val + pb + lane);
             }
-            for (int e0 = 0; e0 < cnt; e0 += kAhead) {
-                double g8[kAhead][kSlabs];
+            for (int e0 = 0; e0 < cnt; e0 += AH) {
+                double g8[AH][S];
 #pragma unroll
-                for (int q = 0; q < kAhead; ++q) {
+                for (int q = 0; q < AH; ++q) {
                     const int col = __shfl_sync(full, ci, min(e0 + q, 31));
                     const double* src = v + static_cast<size_t>(col) * bp + k0 + lane;
 #pragma unroll
-                    for (int s = 0; s < kSlabs; ++s)
+                    for (int s = 0; s < S; ++s)
                         g8[q][s] = (e0 + q < cnt && s < ns) ? __ldg(src + 32 * s) : 0.0;
                 }
 #pragma unroll
-                for (int q = 0; q < kAhead; ++q) {
+                for (int q = 0; q < AH; ++q) {
                     const double a = __shfl_sync(full, ai, min(e0 + q, 31));
                     if (e0 + q < cnt) {
 #pragma unroll
-                        for (int s = 0; s < kSlabs; ++s) acc[s] = dadd(acc[s], dmul(a, g8[q][s]));
+                        for (int s = 0; s < S; ++s) acc[s] = dadd(acc[s], dmul(a, g8[q][s]));
                     }
                 }
             }
         }
 #pragma unroll
-        for (int s = 0; s < kSlabs; ++s)
+        for (int s = 0; s < S; ++s)
             if (s < ns) epi.store(r, k0 + 32 * s + lane, acc[s], epi.load(r, k0 + 32 * s + lane));
     }
 }
@@ -342,11 +349,69 @@ __global__ void k_mark_padding(int batch, int bp, int* __restrict__ done) {
     if (k < bp) done[k] = 1;
 }
 
-template <class Epi>
-int multi_grid(int rows, int groups) {
+template <class Epi, int S, int AH>
+void launch_shape(int rows, int bp, const TileCsr& M, const double* v, const Epi& epi, cudaStream_t st) {
+    if (rows == 0) return;
+    const int groups = (bp + 32 * S - 1) / (32 * S);
     const long long blocks = (static_cast<long long>(rows) * groups + kWarps - 1) / kWarps;
-    return grid_for(reinterpret_cast<const void*>(&k_multi<Epi>), static_cast<int>(std::min<long long>(blocks, 1 << 30)),
-                    0);
+    const int grid = grid_for(reinterpret_cast<const void*>(&k_multi<Epi, S, AH>),
+                              static_cast<int>(std::min<long long>(blocks, 1 << 30)), 0);
+    k_multi<Epi, S, AH><<<grid, kThreads, 0, st>>>(rows, groups, bp, M.ptr, M.idx, M.val, v, epi);
+}
+
+template <class Epi>
+void launch_multi(int shape, int rows, int bp, const TileCsr& M, const double* v, const Epi& epi, cudaStream_t st) {
+    switch (shape) {
+        case 0: launch_shape<Epi, kShapes[0].slabs, kShapes[0].ahead>(rows, bp, M, v, epi, st); break;
+        case 1: launch_shape<Epi, kShapes[1].slabs, kShapes[1].ahead>(rows, bp, M, v, epi, st); break;
+        default: launch_shape<Epi, kShapes[2].slabs, kShapes[2].ahead>(rows, bp, M, v, epi, st); break;
+    }
+}
+
+// Fastest shape for one iteration (dual + primal step) of this matrix at this
+// batch width, timed with CUDA events on the solve's own data (outputs to scratch),
+// cached per (device, matrix, width).
+int autotuned_shape(const TileCsr& A, const TileCsr& AT, int bp, const MultiDualEpi& dual, const double* x_bar,
+                    const MultiPrimalEpi& primal, const double* y, cudaStream_t st) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, const void*, int, int, int>, int> cache;
+    int device = 0;
+    cudaGetDevice(&device);
+    const auto key = std::make_tuple(device, static_cast<const void*>(A.ptr), A.rows, A.nnz, bp);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return 1;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return 1;
+    }
+    int best = 1;
+    float best_ms = 0.f;
+    for (int shape = 0; shape < 3; ++shape) {
+        auto pair = [&]() {
+            launch_multi(shape, A.rows, bp, A, x_bar, dual, st);
+            launch_multi(shape, AT.rows, bp, AT, y, primal, st);
+        };
+        pair();
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 5; ++r) pair();
+        cudaEventRecord(e1, st);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) continue;
+        if (shape == 0 || ms < best_ms) {
+            best = shape;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = best;
+    return best;
 }
 
 }  // namespace
@@ -371,7 +436,7 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
     if (!matrix || batch <= 0 || !c || !rlow || !rupp || !clow || !cupp || !x_out || !results)
         return fail_msg("invalid shared batch arguments");
     if (s.max_iterations <= 0 || s.check_every <= 0 || !(s.primal_tol > 0.0) || !(s.dual_tol > 0.0) ||
-        s.time_limit < 0.0)
+        s.time_limit < 0.0 || s.schedule < 0 || s.schedule > 3)
         return fail_msg("invalid batch settings");
     const int m = matrix->rows, n = matrix->cols;
     if (m < 0 || n <= 0) return fail_msg("invalid matrix dimensions");
@@ -400,13 +465,13 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
     const size_t stage = std::max(NB, MB);
     // batch-minor: x[2], x_bar, cl, cu, (c); y[2], act, (rl, ru); shared: tau, cmass,
     // sig, rmass, (c), (rl, ru); per-LP slots; staging for the layout changes
-    const size_t total = 5 * NB + (c_per_lp ? NB : nb) + 3 * MB + (row_bounds_per_lp ? 2 * MB : 2 * mb) + 2 * nb +
+    const size_t total = 6 * NB + (c_per_lp ? NB : nb) + 3 * MB + (row_bounds_per_lp ? 2 * MB : 2 * mb) + 2 * nb +
                          2 * mb + 12 * kb + stage + 4096;
     DevBuf blob;
     if (blob.alloc(total, "cudaMalloc shared batch workspace")) return -1;
     char* p = blob.as<char>();
     auto take = [&](size_t b) { char* r = p; p += b; return reinterpret_cast<double*>(r); };
-    double *xb0 = take(NB), *xb1 = take(NB), *xbar = take(NB), *dcl = take(NB), *dcu = take(NB);
+    double *xb0 = take(NB), *xb1 = take(NB), *xbar = take(NB), *dcl = take(NB), *dcu = take(NB), *tune = take(NB);
     double* dc = take(c_per_lp ? NB : nb);
     double *yb0 = take(MB), *yb1 = take(MB), *act = take(MB);
     double* drl = take(row_bounds_per_lp ? MB : mb);
@@ -478,10 +543,16 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
         ~Free() { cudaFreeHost(p); }
     } free_host{host_counters};
 
-    const int groups = static_cast<int>((bp + kGroupLps - 1) / kGroupLps);
-    const int grid_d = m ? multi_grid<MultiDualEpi>(m, groups) : 1;
-    const int grid_p = multi_grid<MultiPrimalEpi>(n, groups);
-    const int grid_r = m ? multi_grid<MultiStoreEpi>(m, groups) : 1;
+    int shape = s.schedule - 1;
+    if (s.schedule == 0) {
+        // time on scratch outputs: y_new into the activity buffer, x_new / x_bar into
+        // the staging buffer and the tuning buffer; iterates untouched
+        shape = autotuned_shape(A, AT, bpi,
+                                MultiDualEpi{yb0, drl, dru, sig, done, act, bpi, row_bounds_per_lp ? 1 : 0}, xbar,
+                                MultiPrimalEpi{xb0, dc, tau, dcl, dcu, done, staging, tune, bpi, c_per_lp ? 1 : 0},
+                                yb0, stream);
+        B200_TRY(cudaGetLastError(), "shared batch schedule");
+    }
     const dim3 check_rows(static_cast<unsigned>(std::max(1, std::min((m + 7) / 8, 4 * 148 * 8 * 32 / bpi))), bpi / 32);
     const dim3 check_cols(static_cast<unsigned>(std::max(1, std::min((n + 7) / 8, 4 * 148 * 8 * 32 / bpi))), bpi / 32);
     double* xb[2] = {xb0, xb1};
@@ -497,13 +568,11 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
     int cur = 0, it = 0, launches = 0;
     auto iterate = [&]() {
         const int nx = cur ^ 1;
-        if (m)
-            k_multi<<<grid_d, kThreads, 0, stream>>>(
-                m, groups, bpi, A.ptr, A.idx, A.val, xbar,
-                MultiDualEpi{yb[cur], drl, dru, sig, done, yb[nx], bpi, row_bounds_per_lp ? 1 : 0});
-        k_multi<<<grid_p, kThreads, 0, stream>>>(
-            n, groups, bpi, AT.ptr, AT.idx, AT.val, yb[nx],
-            MultiPrimalEpi{xb[cur], dc, tau, dcl, dcu, done, xb[nx], xbar, bpi, c_per_lp ? 1 : 0});
+        launch_multi(shape, m, bpi, A, xbar, MultiDualEpi{yb[cur], drl, dru, sig, done, yb[nx], bpi,
+                                                           row_bounds_per_lp ? 1 : 0},
+                     stream);
+        launch_multi(shape, n, bpi, AT, yb[nx],
+                     MultiPrimalEpi{xb[cur], dc, tau, dcl, dcu, done, xb[nx], xbar, bpi, c_per_lp ? 1 : 0}, stream);
         cur = nx;
     };
     bool timed_out = false;
@@ -539,8 +608,7 @@ extern "C" int sankhya_b200_shared_batch_pdhg(const SankhyaCudaCSR* matrix, int 
         ++checks;
         B200_TRY(cudaMemsetAsync(counters, 0, 4, stream), "zero counter");
         if (m) {
-            k_multi<<<grid_r, kThreads, 0, stream>>>(m, groups, bpi, A.ptr, A.idx, A.val, xb[cur],
-                                                     MultiStoreEpi{act, bpi});
+            launch_multi(shape, m, bpi, A, xb[cur], MultiStoreEpi{act, bpi}, stream);
             k_multi_rows_check<<<check_rows, tblock, 0, stream>>>(m, bpi, row_bounds_per_lp ? 1 : 0, act, yb[cur],
                                                                   yb[cur ^ 1], drl, dru, done, viol, dstep);
         }
