@@ -62,6 +62,28 @@ def test_deterministic_and_parameters_roundtrip(engine, instances):
         other.set_parameters(bad)
 
 
+def test_rejects_invalid_inputs(engine, instances):
+    inst = _instance(instances)
+    A = engine.Matrix.from_instance(inst)
+    net = engine.Gnn(seed=2)
+    before = net.parameters()
+    bad = dict(inst)
+    bad["c"] = inst["c"].copy()
+    bad["c"][3] = np.nan
+    with pytest.raises(RuntimeError, match="cost or column bound"):
+        net.predict(A, bad)
+    bad = dict(inst)
+    bad["rl"] = inst["rl"].copy()
+    bad["rl"][2] = inst["ru"][2] + 1.0
+    with pytest.raises(RuntimeError, match="row bound"):
+        net.train_step(A, bad, np.zeros(inst["n"]), np.zeros(inst["m"]))
+    xt = np.zeros(inst["n"])
+    xt[0] = np.inf
+    with pytest.raises(RuntimeError, match="training target"):
+        net.train_step(A, inst, xt, np.zeros(inst["m"]))
+    assert np.array_equal(net.parameters(), before)   # nothing was applied
+
+
 def test_prediction_inside_bounds(engine, instances):
     inst = _instance(instances)
     A = engine.Matrix.from_instance(inst)

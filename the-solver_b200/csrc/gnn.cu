@@ -729,6 +729,13 @@ int prepare(SankhyaB200Gnn* g, const SankhyaCudaCSR* matrix, const double* c, co
     if (check_model(g)) return -1;
     if (!matrix || !c || !cl || !cu || ((!rl || !ru) && matrix->rows > 0)) return fail_msg("invalid network arguments");
     if (matrix->cols <= 0 || matrix->rows < 0) return fail_msg("invalid matrix dimensions");
+    // the checks of sankhya_b200_pdlp_solve: a NaN would poison the features and,
+    // through a training step, the parameters
+    for (int j = 0; j < matrix->cols; ++j)
+        if (!std::isfinite(c[j]) || std::isnan(cl[j]) || std::isnan(cu[j]) || cl[j] > cu[j])
+            return fail_msg("invalid cost or column bound");
+    for (int i = 0; i < matrix->rows; ++i)
+        if (std::isnan(rl[i]) || std::isnan(ru[i]) || rl[i] > ru[i]) return fail_msg("invalid row bound");
     if (get_plan(matrix, plan)) return -1;
     if (ensure_workspace(g, matrix->rows, matrix->cols)) return -1;
     return upload_instance(g, **plan, c, rl, ru, cl, cu, engine_stream());
@@ -736,6 +743,10 @@ int prepare(SankhyaB200Gnn* g, const SankhyaCudaCSR* matrix, const double* c, co
 
 int upload_targets(SankhyaB200Gnn* g, int m, int n, const double* x_t, const double* y_t, cudaStream_t st) {
     if (!x_t || (m > 0 && !y_t)) return fail_msg("missing training targets");
+    for (int j = 0; j < n; ++j)
+        if (!std::isfinite(x_t[j])) return fail_msg("non-finite training target");
+    for (int i = 0; i < m; ++i)
+        if (!std::isfinite(y_t[i])) return fail_msg("non-finite training target");
     B200_TRY(cudaMemcpyAsync(g->x_t, x_t, 8LL * n, cudaMemcpyHostToDevice, st), "upload x target");
     if (m) B200_TRY(cudaMemcpyAsync(g->y_t, y_t, 8LL * m, cudaMemcpyHostToDevice, st), "upload y target");
     return 0;
