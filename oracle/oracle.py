@@ -349,6 +349,55 @@ def ref_sk_verify(inst, x, y, quadratic=False):
                 "dual_infeasibility": s.dual_infeasibility, "complementarity": s.complementarity}
 
 
+def ref_read_mps(path):
+    """The reference's own MPS/QPS reader (sk_read_mps, c/src/sk_core.c): the model as
+    an instance dict (A in CSR with ascending columns per row, the counting-sort order of
+    the reference's apps/*.cu csc_to_csr), plus Q as full symmetric CSR when present.
+    Infinite bounds come back as +-inf (the reader's 1e30 sentinels converted)."""
+    lib = load("ref")
+    model = SkModel()
+    lib.sk_model_init(C.byref(model))
+    st = lib.sk_read_mps(path.encode(), C.byref(model))
+    if st != 0:
+        lib.sk_model_free(C.byref(model))
+        raise ValueError(f"sk_read_mps({path}) returned {st}")
+    try:
+        m, n = model.nrow, model.ncol
+        nnz = model.A.p[n]
+        cp = np.ctypeslib.as_array(model.A.p, (n + 1,)).copy()
+        ci = np.ctypeslib.as_array(model.A.i, (nnz,)).copy() if nnz else np.zeros(0, np.int32)
+        cx = np.ctypeslib.as_array(model.A.x, (nnz,)).copy() if nnz else np.zeros(0)
+
+        def csr(rows_, cols_, p_, i_, x_):
+            cnt = np.bincount(i_, minlength=rows_) if len(i_) else np.zeros(rows_, np.int64)
+            ptr = np.zeros(rows_ + 1, np.int32)
+            np.cumsum(cnt, out=ptr[1:])
+            col = np.repeat(np.arange(cols_, dtype=np.int32), np.diff(p_))
+            order = np.argsort(i_, kind="stable")
+            return ptr, col[order].astype(np.int32), x_[order].copy()
+
+        def vec(ptr_, k):
+            v = np.ctypeslib.as_array(ptr_, (k,)).copy() if k else np.zeros(0)
+            v[v >= 1e30] = np.inf
+            v[v <= -1e30] = -np.inf
+            return v
+
+        ptr, idx, val = csr(m, n, cp, ci, cx)
+        inst = dict(m=m, n=n, ptr=ptr, idx=idx, val=val, c=vec(model.c, n), rl=vec(model.rlow, m),
+                    ru=vec(model.rupp, m), cl=vec(model.clow, n), cu=vec(model.cupp, n),
+                    objshift=model.objshift,
+                    integer=np.ctypeslib.as_array(model.vartype, (n,)).copy() if n else np.zeros(0, np.uint8))
+        if model.Q:
+            q = model.Q.contents
+            qn = q.p[n]
+            qp = np.ctypeslib.as_array(q.p, (n + 1,)).copy()
+            inst["q_ptr"], inst["q_idx"], inst["q_val"] = csr(
+                n, n, qp, np.ctypeslib.as_array(q.i, (qn,)).copy(), np.ctypeslib.as_array(q.x, (qn,)).copy())
+        return inst
+    finally:
+        lib.sk_model_free(C.byref(model))
+
+
 def ref_sk_scale_model(inst, passes=4):
     lib = load("ref")
     keep = _Keep()
