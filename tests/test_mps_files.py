@@ -121,3 +121,39 @@ def test_app_steps_follow_column_order():
     col = A.sum(axis=0) + np.abs(inst["Q"]).sum(axis=0)
     np.testing.assert_allclose(primal, 0.9 / (1 + col), rtol=1e-15)
     np.testing.assert_allclose(dual, 0.9 / (1 + A.sum(axis=1)), rtol=1e-15)
+
+
+SMOKE = os.path.join(ROOT, "oracle", "_ref", "smoke")
+needs_smoke = pytest.mark.skipif(not os.path.isdir(SMOKE), reason="reference CLI model files not copied")
+
+
+@needs_ref
+@needs_smoke
+def test_cli_model_files_known_answers(oracle):
+    """The reference's CLI model files (bench/smoke/, run by cuda/CMakeLists.txt:31-48)
+    read through its own reader, solved by the oracle with the programs' steps and
+    settings: the known answers the gpu runs of those programs are held to."""
+    unit = oracle.ref_read_mps(os.path.join(SMOKE, "unit_lp.mps"))
+    step = 0.5 / oracle.power_norm(unit, 30)
+    rc, x, _, r = oracle.fixed_pdhg(unit, dict(APP_SETTINGS, max_iterations=5000, tolerance=1e-5, tau=step,
+                                               sigma=step), want_dual=False)
+    assert rc == 0 and r["status"] == 0 and abs(x[0] - 1.0) <= 1e-5 and abs(r["objective"] - 1.0) <= 1e-5
+
+    tiny = oracle.ref_read_mps(os.path.join(SMOKE, "tiny_lp.mps"))
+    step = 0.5 / oracle.power_norm(tiny, 30)
+    rc, x, _, r = oracle.fixed_pdhg(tiny, dict(APP_SETTINGS, tau=step, sigma=step), want_dual=False)
+    assert rc == 0 and r["status"] == 0
+    assert np.allclose(x, [3.0, 1.0], atol=1e-6) and abs(r["objective"] + 11.0) <= 1e-6
+
+    qp = oracle.ref_read_mps(os.path.join(SMOKE, "tiny_qp.qps"))
+    assert mf.q_diagonal(qp) is None and np.diff(qp["ptr"]).sum() == 1
+    primal, dual = mf.app_qp_steps(qp)
+    rc, x, y, r = oracle.fixed_pdhg(qp, dict(APP_SETTINGS, max_iterations=100000, tolerance=1e-5, tau=0.0,
+                                             sigma=0.0), primal_steps=primal, dual_steps=dual, hessian=True)
+    assert rc == 0 and r["status"] == 0 and np.allclose(x, [2.0, 0.0], atol=1e-5)
+    assert abs(r["objective"] + 4.0) <= 1e-5
+    st, v = oracle.ref_sk_verify(qp, x, y, quadratic=True)
+    assert st == 0 and max(v["primal_infeasibility"], v["dual_infeasibility"], v["complementarity"]) <= 1e-3
+
+    with pytest.raises(ValueError):   # no constraint rows: the reader rejects the guard's file
+        oracle.ref_read_mps(os.path.join(SMOKE, "nonconvex_qp.qps"))
