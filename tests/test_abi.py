@@ -48,6 +48,23 @@ def test_no_device_is_a_clean_error(engine):
     assert rc != 0 and "device" in engine.last_error().lower()
 
 
+def test_host_spmv_rejects_out_of_bounds_csr_before_device_work(engine):
+    """sankhya_cuda_spmv_f64 checks, on the host and before any device query, what
+    would send its kernel outside the uploaded buffers: offsets outside [0, nnz],
+    decreasing offsets, columns outside [0, cols). Runs the same with or without a GPU."""
+    vals, x = [1.0, 2.0, 3.0, 4.0], [2.0, 5.0, 7.0]
+    rc, _ = engine.spmv_host(2, 3, [0, 2, 5], [0, 2, 1, 2], vals, x)
+    assert rc == -1 and "row-offset endpoints" in engine.last_error()
+    rc, _ = engine.spmv_host(2, 3, [-1, 2, 4], [0, 2, 1, 2], vals, x)
+    assert rc == -1 and "row-offset endpoints" in engine.last_error()
+    rc, _ = engine.spmv_host(2, 3, [0, 3, 2], [0, 2, 1, 2], vals, x)
+    assert rc == -1 and "row-offset ordering" in engine.last_error()
+    rc, _ = engine.spmv_host(2, 3, [0, 2, 4], [0, 3, 1, 2], vals, x)
+    assert rc == -1 and "column index" in engine.last_error()
+    rc, _ = engine.spmv_host(2, 3, [0, 2, 4], [0, 2, -1, 2], vals, x)
+    assert rc == -1 and "column index" in engine.last_error()
+
+
 def test_every_solver_entry_fails_without_a_device(engine, instances):
     """No host path behind any solver entry point: without a GPU each returns -1 with
     an error text (checked where this suite runs without one)."""

@@ -76,6 +76,15 @@ extern "C" int sankhya_cuda_spmv_f64(int rows, int cols, int nnz, const int* row
         (nnz > 0 && (column_indices == nullptr || values == nullptr)) || (cols > 0 && x == nullptr))
         return fail_msg("null CSR or vector pointer");
     if (rows == 0) return 0;
+    // The reference launches on these arrays unchecked. An offset outside [0, nnz],
+    // decreasing offsets or a column outside [0, cols) would send the kernel outside
+    // its buffers, so those (and only those) are rejected here, before any device work;
+    // every input the reference reads in bounds behaves as there.
+    if (row_offsets[0] < 0 || row_offsets[rows] > nnz) return fail_msg("invalid CSR row-offset endpoints");
+    for (int r = 0; r < rows; ++r)
+        if (row_offsets[r] > row_offsets[r + 1]) return fail_msg("invalid CSR row-offset ordering");
+    for (int p = row_offsets[0]; p < row_offsets[rows]; ++p)
+        if (column_indices[p] < 0 || column_indices[p] >= cols) return fail_msg("invalid CSR column index");
     if (ensure_device()) return -1;
     std::vector<int> tiles = build_tiles(rows, row_offsets);
     DevBuf d_ptr, d_idx, d_val, d_x, d_y, d_tiles;
