@@ -107,7 +107,8 @@ typedef struct SankhyaB200LoopResult {
    QP the sk_verify score <= 100 (primal_tol + 2 dual_tol)). x (ncol), y (nrow) and
    activity (nrow) are host outputs with the reference's meaning. The time limit
    is tested after every 20-iteration window instead of after every iteration.
-   Returns 0, SK_ERR_ARG (1) on invalid input, SK_ERR_MEMORY (2) on allocation
+   Returns 0, SK_ERR_ARG (1) on invalid input (including a model that
+   sk_model_validate rejects, vartype aside), SK_ERR_MEMORY (2) on allocation
    failure, SK_ERR_NUMERIC (7) on a CUDA error. */
 SANKHYA_CUDA_API int sankhya_b200_pdhg_loop(
     const sk_model* model, const sk_options* options, double* x, double* y,

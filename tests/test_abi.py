@@ -97,3 +97,82 @@ def test_every_solver_entry_fails_without_a_device(engine, instances):
     rc = L.sankhya_b200_pdlp_solve(C.byref(fake), d(inst["c"]), d(inst["rl"]), d(inst["ru"]), d(inst["cl"]),
                                    d(inst["cu"]), C.byref(ps), None, None, d(x), None, C.byref(pr))
     assert rc == -1 and "device" in engine.last_error().lower()
+
+
+def test_loop_hook_validates_the_model_before_device_work(engine, oracle, instances):
+    """sankhya_b200_pdhg_loop applies sk_model_validate's checks (c/src/sk_core.c:126-155)
+    before any device call: each malformed variant returns SK_ERR_ARG (1). Without a
+    GPU, the well-formed models the gpu tests solve get past them and stop at the
+    device check (SK_ERR_NUMERIC, 7), so the checks reject none of those."""
+    import ctypes as C
+    import json
+    import numpy as np
+    import torch
+    L = engine.lib()
+
+    def call(inst, quadratic=False, edit=None):
+        keep = oracle._Keep()
+        model = oracle.build_sk_model(keep, inst, quadratic)
+        if edit:
+            edit(model, keep)
+        opts = oracle.SkOptions(primal_tol=1e-6, dual_tol=1e-6, iteration_limit=100, threads=1)
+        x, y, act = np.zeros(inst["n"]), np.zeros(inst["m"]), np.zeros(inst["m"])
+        res = engine.LoopResult()
+        return L.sankhya_b200_pdhg_loop(C.byref(model), C.byref(opts), engine._p(x), engine._p(y), engine._p(act),
+                                        C.byref(res))
+
+    lp = instances.lp_uniform(12, 60, 150, 4)
+    qp = instances.qp_diag_plus_lowrank(3, 40, 80, a_per_col=4, l_per_col=2)
+    if not torch.cuda.is_available():
+        man = json.load(open(os.path.join(ROOT, "tests", "golden", "manifest.json")))
+        for name, seed, m, n, per_col, limits in man["lp"]:
+            assert call(instances.lp_uniform(seed, m, n, per_col)) == 7, name
+        assert call(lp) == 7 and call(qp, quadratic=True) == 7
+
+    def setp(k, v):
+        def edit(model, keep):
+            arr = np.ctypeslib.as_array(model.A.p, (model.ncol + 1,)).copy()
+            arr[k] = v
+            model.A.p = oracle._p(keep.i(arr), oracle.iptr)
+        return edit
+
+    def seti(k, v):
+        def edit(model, keep):
+            nnz = model.A.p[model.ncol]
+            arr = np.ctypeslib.as_array(model.A.i, (nnz,)).copy()
+            arr[k] = v
+            model.A.i = oracle._p(keep.i(arr), oracle.iptr)
+        return edit
+
+    def setd(field, k, v):
+        def edit(model, keep):
+            size = model.ncol if field in ("c", "clow", "cupp") else model.nrow
+            arr = np.ctypeslib.as_array(getattr(model, field), (size,)).copy()
+            arr[k] = v
+            setattr(model, field, oracle._p(keep.d(arr)))
+        return edit
+
+    nnz = int(lp["ptr"][-1])
+    bad = [
+        setp(0, 1),                                    # p[0] != 0
+        setp(5, 10 ** 6),                              # offset beyond nnz
+        setp(lp["n"], nnz + 1),                        # p[ncol] beyond nzmax
+        seti(3, lp["m"]),                              # row index out of range
+        seti(0, -1),
+        setd("c", 2, float("nan")),                    # non-finite cost
+        setd("clow", 1, 20.0),                         # crossed column bound (upper 10)
+        setd("rlow", 0, float("nan")),                 # NaN row bound
+        lambda model, keep: setattr(model.A, "nzmax", nnz - 1),   # nnz beyond nzmax
+        lambda model, keep: setattr(model.A, "nrow", lp["m"] + 1),
+    ]
+    for k, edit in enumerate(bad):
+        assert call(lp, edit=edit) == 1, k
+        assert "invalid sk model" in engine.last_error(), k
+
+    def bad_q(model, keep):
+        q = model.Q.contents
+        n = q.ncol
+        arr = np.ctypeslib.as_array(q.i, (q.p[n],)).copy()
+        arr[0] = n
+        q.i = oracle._p(keep.i(arr), oracle.iptr)
+    assert call(qp, quadratic=True, edit=bad_q) == 1

@@ -868,6 +868,32 @@ extern "C" int sankhya_cuda_qp_pdhg_preconditioned_with_dual(
                        primal_steps, dual_steps, solution, dual_solution, result);
 }
 
+// What sk_model_validate requires of a model (c/src/sk_core.c:126-155), except
+// vartype, which the loop never reads: a well-formed CSC for A (and Q) and finite
+// costs with ordered, non-NaN bounds. sk_solve checks this before its loop; this
+// entry checks it again because its host setup and device schedules index through
+// the CSC arrays.
+static bool sk_csc_ok(const sk_csc* a, int rows, int cols) {
+    if (!a || a->nrow != rows || a->ncol != cols || a->nzmax < 0 || !a->p || a->p[0] != 0) return false;
+    const int nnz = a->p[cols];
+    if (nnz < 0 || nnz > a->nzmax || (nnz > 0 && (!a->i || !a->x))) return false;
+    for (int j = 0; j < cols; ++j)
+        if (a->p[j] > a->p[j + 1] || a->p[j + 1] > nnz) return false;
+    for (int p = 0; p < nnz; ++p)
+        if (a->i[p] < 0 || a->i[p] >= rows || !std::isfinite(a->x[p])) return false;
+    return true;
+}
+
+static bool sk_model_ok(const sk_model* m) {
+    if (!sk_csc_ok(&m->A, m->nrow, m->ncol) || (m->Q && !sk_csc_ok(m->Q, m->ncol, m->ncol))) return false;
+    for (int j = 0; j < m->ncol; ++j)
+        if (!std::isfinite(m->c[j]) || std::isnan(m->clow[j]) || std::isnan(m->cupp[j]) || m->clow[j] > m->cupp[j])
+            return false;
+    for (int i = 0; i < m->nrow; ++i)
+        if (std::isnan(m->rlow[i]) || std::isnan(m->rupp[i]) || m->rlow[i] > m->rupp[i]) return false;
+    return true;
+}
+
 extern "C" int sankhya_b200_pdhg_loop(const sk_model* model, const sk_options* options, double* x, double* y,
                                       double* activity, SankhyaB200LoopResult* result) {
     clear_error();
@@ -880,6 +906,10 @@ extern "C" int sankhya_b200_pdhg_loop(const sk_model* model, const sk_options* o
         !model->A.p || (model->Q && (!model->Q->p || model->Q->nrow != n || model->Q->ncol != n)) ||
         options->primal_tol <= 0.0 || options->dual_tol <= 0.0) {
         fail_msg("invalid sk loop arguments");
+        return 1;
+    }
+    if (!sk_model_ok(model)) {
+        fail_msg("invalid sk model (malformed CSC, non-finite cost, or NaN / crossed bound)");
         return 1;
     }
     int devices = 0;
