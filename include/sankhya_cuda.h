@@ -3,7 +3,7 @@
  * Symbol-for-symbol replacement for the reference's cuda/include/sankhya_cuda.h:
  * the same function names, argument meaning, return codes and struct layouts, so
  * an application linked against the reference library (apps/sankhya_pdhg.cu,
- * apps/sankhya_qp_cuda.cu, cuda/tests/*.cu) links against libsankhya_cuda.so
+ * apps/sankhya_qp_cuda.cu, the cuda/tests programs) links against libsankhya_cuda.so
  * built here without source changes. Each declaration cites the reference
  * declaration it replaces (path relative to the reference project).
  *
