@@ -145,7 +145,8 @@ enum {
 };
 
 typedef struct SankhyaB200PdlpSettings {
-    int struct_version;   /* 3 (2: without initial_primal_weight; 1: also without algorithm) */
+    int struct_version;   /* 4 (3: without cancel / cancel_context; 2: also without
+                             initial_primal_weight; 1: also without algorithm)       */
     int max_iterations;   /* total PDHG iterations (accepted + rejected)          */
     int restart_period;   /* iterations between evaluations (GpuPdlp: 64)         */
     int power_iterations; /* power iterations for ||A||_2 (GpuPdlp: 30)           */
@@ -162,12 +163,19 @@ typedef struct SankhyaB200PdlpSettings {
     int reserved;
     double initial_primal_weight; /* > 0: start from this primal weight (e.g. one learned
                                      for an LP family); 0: ||c|| / ||b|| (version 3)      */
+    int (*cancel)(void* context); /* non-NULL: called once per restart window, where the
+                                     host synchronizes anyway, on the calling thread; a
+                                     non-zero return stops the solve with status 3
+                                     (GpuPdlp's PdlpParams::cancel, polled the same way,
+                                     src/cuda/GpuPdlp.hpp:62-67) (version 4)              */
+    void* cancel_context;         /* passed to cancel (version 4)                         */
 } SankhyaB200PdlpSettings;
 
 SANKHYA_CUDA_API void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* settings);
 
 typedef struct SankhyaB200PdlpResult {
-    int status;            /* 0 converged, 1 iteration limit, 2 time limit, -2 numeric */
+    int status;            /* 0 converged, 1 iteration limit, 2 time limit, 3 cancelled,
+                              -2 numeric                                              */
     int iterations;
     int restarts;
     int rejected_steps;

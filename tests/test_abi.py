@@ -176,3 +176,65 @@ def test_loop_hook_validates_the_model_before_device_work(engine, oracle, instan
         arr[0] = n
         q.i = oracle._p(keep.i(arr), oracle.iptr)
     assert call(qp, quadratic=True, edit=bad_q) == 1
+
+
+MIRRORS = {  # ctypes class in the package -> C struct in include/
+    "CSR": "SankhyaCudaCSR", "Settings": "SankhyaCudaLPSettings", "Result": "SankhyaCudaLPResult",
+    "Timing": "SankhyaB200Timing", "LoopResult": "SankhyaB200LoopResult",
+    "PdlpSettings": "SankhyaB200PdlpSettings", "PdlpResult": "SankhyaB200PdlpResult",
+    "BatchSettings": "SankhyaB200BatchSettings", "BatchResult": "SankhyaB200BatchResult",
+    "GnnSettings": "SankhyaB200GnnSettings",
+}
+
+
+def test_ctypes_mirrors_match_the_headers(engine, tmp_path):
+    """Every ctypes mirror has the size and field offsets the C compiler gives the
+    header's struct (a program built against include/ prints them)."""
+    import subprocess
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "sankhya_cuda.h"', '#include "sankhya_b200.h"',
+             "int main(void) {"]
+    for py, cs in MIRRORS.items():
+        cls = getattr(engine, py)
+        lines.append(f'printf("{py} size %zu\\n", sizeof({cs}));')
+        for name, _ in cls._fields_:
+            lines.append(f'printf("{py} {name} %zu\\n", offsetof({cs}, {name}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    r = subprocess.run(["gcc", "-std=c11", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        py, name, value = line.split()
+        got[(py, name)] = int(value)
+    for py in MIRRORS:
+        cls = getattr(engine, py)
+        assert C.sizeof(cls) == got[(py, "size")], py
+        for name, _ in cls._fields_:
+            assert getattr(cls, name).offset == got[(py, name)], (py, name)
+
+
+def test_pdlp_settings_versions(engine, instances):
+    """Settings versions 1 to 4 pass the settings checks (they stop at the device check
+    here); other versions are refused. Version 3 callers' structs end before `cancel`,
+    version 2 before `initial_primal_weight`, version 1 before `algorithm`."""
+    import numpy as np
+    import torch
+    if torch.cuda.is_available():
+        return
+    inst = instances.lp_uniform(1, 8, 12, 2)
+    fake = engine.CSR(inst["m"], inst["n"], int(inst["ptr"][-1]), None, None, None)
+    L = engine.lib()
+    d = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double))
+    s = engine.pdlp_default_settings()
+    assert s.struct_version == 4 and not s.cancel
+    for version, message in ((1, "device"), (2, "device"), (3, "device"), (4, "device"), (0, "struct_version"),
+                             (5, "struct_version")):
+        s.struct_version = version
+        res = engine.PdlpResult()
+        x = np.zeros(inst["n"])
+        rc = L.sankhya_b200_pdlp_solve(C.byref(fake), d(inst["c"]), d(inst["rl"]), d(inst["ru"]), d(inst["cl"]),
+                                       d(inst["cu"]), C.byref(s), None, None, d(x), None, C.byref(res))
+        assert rc == -1 and message in engine.last_error(), (version, engine.last_error())

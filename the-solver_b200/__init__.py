@@ -115,7 +115,7 @@ class PdlpSettings(C.Structure):
                 ("ruiz_iterations", C.c_int), ("precision", C.c_int), ("eps_optimal", C.c_double),
                 ("time_limit", C.c_double), ("eta_min_factor", C.c_double), ("eta_max_factor", C.c_double),
                 ("ruiz_tolerance", C.c_double), ("algorithm", C.c_int), ("reserved", C.c_int),
-                ("initial_primal_weight", C.c_double)]
+                ("initial_primal_weight", C.c_double), ("cancel", C.c_void_p), ("cancel_context", C.c_void_p)]
 
 
 class PdlpResult(C.Structure):

@@ -898,12 +898,14 @@ struct LoopParams {
     double omega0 = 0.0;  // > 0: initial primal weight (else ||c|| / ||b||)
     double eta0 = 0.0;    // > 0: initial step size (else 0.9 / ||A||_2)
     bool halpern = false; // reflected restarted Halpern PDHG instead of GpuPdlp's loop
+    int (*cancel)(void*) = nullptr;  // polled after each window; non-zero stops the solve
+    void* cancel_context = nullptr;
 };
 
 struct LoopStats {
     long long iterations = 0;
     int restarts = 0, syncs = 0;
-    bool converged = false, timed_out = false, numeric = false;
+    bool converged = false, timed_out = false, numeric = false, cancelled = false;
     double eta = 0.0, accept_count = 0.0, updates = 0.0, omega = 1.0;
     Kkt best;
 };
@@ -1140,6 +1142,10 @@ struct Core {
                 out->timed_out = true;
                 break;
             }
+            if (lp.cancel && lp.cancel(lp.cancel_context) != 0) {
+                out->cancelled = true;
+                break;
+            }
             const double r = std::sqrt(omega * dx2 + dy2 / omega);
             const bool sufficient = r <= kSufficient * r_restart;
             const bool necessary = r <= kNecessary * r_restart && r > r_previous;
@@ -1247,6 +1253,10 @@ struct Core {
                 out->timed_out = true;
                 break;
             }
+            if (lp.cancel && lp.cancel(lp.cancel_context) != 0) {
+                out->cancelled = true;
+                break;
+            }
             const double mu = best.worst();
             const bool sufficient = mu <= kSufficient * mu_at_restart;
             const bool necessary = mu <= kNecessary * mu_at_restart && mu > mu_previous;
@@ -1289,7 +1299,7 @@ using namespace b200;
 extern "C" void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* s) {
     if (!s) return;
     std::memset(s, 0, sizeof(*s));
-    s->struct_version = 3;
+    s->struct_version = 4;
     s->max_iterations = 500000;
     s->restart_period = 64;
     s->power_iterations = 30;
@@ -1321,12 +1331,14 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         } else if (settings->struct_version == 2) {
             std::memcpy(&s, settings, offsetof(SankhyaB200PdlpSettings, initial_primal_weight));
         } else if (settings->struct_version == 3) {
+            std::memcpy(&s, settings, offsetof(SankhyaB200PdlpSettings, cancel));
+        } else if (settings->struct_version == 4) {
             s = *settings;
         } else {
             return fail_msg("unsupported settings struct_version");
         }
     }
-    s.struct_version = 3;
+    s.struct_version = 4;
     if (s.algorithm != SANKHYA_B200_PDLP_ADAPTIVE && s.algorithm != SANKHYA_B200_PDLP_HALPERN)
         return fail_msg("invalid PDLP settings");
     if (!(s.initial_primal_weight >= 0.0) || !std::isfinite(s.initial_primal_weight))
@@ -1384,6 +1396,8 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     lp.halpern = s.algorithm == SANKHYA_B200_PDLP_HALPERN;
     if (s.initial_primal_weight > 0.0) lp.omega0 = std::min(kMaxWeight, std::max(kMinWeight, s.initial_primal_weight));
     lp.deadline = s.time_limit > 0.0 ? t_start + s.time_limit : 0.0;
+    lp.cancel = s.cancel;
+    lp.cancel_context = s.cancel_context;
     lp.matrix_norm = matrix_norm;
     lp.eta_min_factor = s.eta_min_factor;
     lp.eta_max_factor = s.eta_max_factor;
@@ -1450,7 +1464,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         stats = fs;
         k_widen<<<gv, kThreads, 0, stream>>>(n, m, lo.x, lo.y, sc.cl, sc.cu, hi.x, hi.y);
         const long long left = s.max_iterations - fs.iterations;
-        if (!fs.numeric && !fs.timed_out && left > 0 && (!fs.converged || s.eps_optimal < flp.eps)) {
+        if (!fs.numeric && !fs.timed_out && !fs.cancelled && left > 0 && (!fs.converged || s.eps_optimal < flp.eps)) {
             lp.eps = s.eps_optimal;
             lp.max_iterations = left;
             lp.cost_norm = cost_norm;
@@ -1471,6 +1485,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
             stats.converged = fin.converged;
             stats.timed_out = fin.timed_out;
             stats.numeric = fin.numeric;
+            stats.cancelled = fin.cancelled;
         }
         launches += hi.launches + lo.launches;
     }
@@ -1483,7 +1498,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     ++syncs;
     syncs += stats.syncs;
     const Kkt& best = stats.best;
-    result->status = stats.numeric ? -2 : stats.converged ? 0 : stats.timed_out ? 2 : 1;
+    result->status = stats.numeric ? -2 : stats.converged ? 0 : stats.cancelled ? 3 : stats.timed_out ? 2 : 1;
     result->iterations = static_cast<int>(std::min<long long>(stats.iterations, 2147483647LL));
     result->restarts = stats.restarts;
     result->rejected_steps = (lp.adaptive && !lp.halpern)
