@@ -201,12 +201,24 @@ def time_to_kkt(E, A, inst, eps=1e-6, limit_s=90.0):
         rc, x, y, r = E.pdlp_solve(A, inst, s)
         wall = time.perf_counter() - t0
         out[name] = {"seconds": round(wall, 3), "status": r["status"], "iterations": r["iterations"],
-                     "refinements": r["refinements"], "objective": float(np.dot(inst["c"], x)),
-                     "kkt": [r["relative_primal_residual"], r["relative_dual_residual"], r["relative_gap"]]}
+                     "refinements": r["refinements"], "objective": _finite(np.dot(inst["c"], x)),
+                     "kkt": [_finite(r[k]) for k in ("relative_primal_residual", "relative_dual_residual",
+                                                     "relative_gap")]}
+    ref_obj = out["fp64"]["objective"]
     for name in ("fp32_refined", "halpern_fp64", "halpern_fp32_refined"):
-        if out["fp64"]["status"] == 0 and out[name]["status"] == 0:
+        if out["fp64"]["status"] == 0 and out[name]["status"] == 0 and out[name]["seconds"] > 0:
             out[f"speedup_{name}_vs_fp64"] = round(out["fp64"]["seconds"] / out[name]["seconds"], 3)
+        # the accuracy side of the target: objective against the FP64 run's, relative
+        obj = out[name]["objective"]
+        out[name]["objective_rel_diff_vs_fp64"] = (
+            None if obj is None or ref_obj is None else _finite(abs(obj - ref_obj) / (1.0 + abs(ref_obj))))
     return out
+
+
+def _finite(v):
+    """A float for the JSON line, or None where it is not finite (NaN is not JSON)."""
+    v = float(v)
+    return v if np.isfinite(v) else None
 
 
 def run_reference(args, world, rank):
