@@ -77,3 +77,22 @@ def test_time_to_kkt_survives_instant_solves():
     out = b.time_to_kkt(E, None, {"c": np.array([1.0])})
     assert all(out[k]["objective_rel_diff_vs_fp64"] == 0.0 for k in ("fp32_refined", "halpern_fp64"))
     json.dumps(out, allow_nan=False)
+
+
+def test_clock_summary_parses_nvidia_smi_rows():
+    """The clocks record: median SM clock under load, the maximum, and the throttle
+    reasons that were Active in any sample (nvidia-smi csv, noheader, nounits)."""
+    b = _bench()
+    sampler = b.ClockSampler(0)
+    sampler.out = "\n".join([
+        "0, 1965, 1965, 612.3, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "0, 1950, 1965, 998.1, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "0, 1965, 1965, 700.0, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "garbage line",
+    ])
+    s = sampler.summary()
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"] and s["samples"] == 3
+    empty = b.ClockSampler(0)
+    empty.out = ""
+    assert empty.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
