@@ -22,8 +22,9 @@ Algorithmic bytes of one iteration (each vector element and nonzero once):
   A'-side launch: 12 nnz + 4 (n+1) + 8 m (y_new gather) + 48 n (x, c, cl, cu, x_new, x_bar)
 
 --impl reference runs the reference's own CPU PDHG (sk_solve with
-lp_engine = SK_LP_FIRST_ORDER from its C sources, oracle/_ref) on the same
-instance and reports the same metric over its loop time.
+lp_engine = SK_LP_FIRST_ORDER from its C sources, oracle/_ref, the OpenMP build on
+every core this process may use) on the same instance and reports the same metric
+over its loop time.
 Multi-GPU: replicas only (one independent instance per rank, no exchange).
 """
 from __future__ import annotations
@@ -162,12 +163,27 @@ def job_throughput(world, bytes_per_unit, units_per_rank, seconds_max):
     return world * bytes_per_unit * units_per_rank / seconds_max / 1e9
 
 
-def reference_loop_gbs(inst, iterations):
-    """The reference's sk_solve (SK_LP_FIRST_ORDER) for `iterations` iterations;
-    returns (GB/s over its loop time, loop seconds)."""
+def reference_core():
+    """(library, threads) for the timed runs of the reference's C core: its OpenMP build
+    (threaded csc_tmv, the same bits) on every core this process may use, or, where
+    that build or its OpenMP runtime is missing, the serial build on one."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    st, out = O.ref_sk_solve(inst, primal_tol=1e-300, dual_tol=1e-300, iteration_limit=iterations)
+    try:
+        O.load("ref_omp")
+        return "ref_omp", len(os.sched_getaffinity(0))
+    except OSError:
+        return "ref", 1
+
+
+def reference_loop_gbs(inst, iterations, core=("ref", 1)):
+    """The reference's sk_solve (SK_LP_FIRST_ORDER) for `iterations` iterations;
+    returns (GB/s over its loop time, loop seconds, iterations)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    lib_name, threads = core
+    st, out = O.ref_sk_solve(inst, lib_name=lib_name, threads=threads, primal_tol=1e-300, dual_tol=1e-300,
+                             iteration_limit=iterations)
     if st != 0:
         raise RuntimeError(f"reference sk_solve failed with status {st}")
     secs = out["solve_seconds"]
@@ -175,14 +191,21 @@ def reference_loop_gbs(inst, iterations):
     return iteration_bytes(inst["m"], inst["n"], nnz) * out["iterations"] / secs / 1e9, secs, out["iterations"]
 
 
+def _core_text(core):
+    lib_name, threads = core
+    return (f"{threads} threads, the reference's c/src built with OpenMP" if lib_name == "ref_omp"
+            else "1 thread, the reference's c/src built without OpenMP")
+
+
 def cpu_baseline(inst, target_seconds=12.0):
     """Bounded sample of the reference CPU PDHG on this instance (rank 0, N=1)."""
-    gbs1, secs1, it1 = reference_loop_gbs(inst, 1)
+    core = reference_core()
+    gbs1, secs1, it1 = reference_loop_gbs(inst, 1, core)
     iters = int(max(2, min(200, target_seconds / max(secs1, 1e-3))))
-    gbs, secs, its = reference_loop_gbs(inst, iters)
-    return {"value": round(gbs, 4), "unit": "GB/s", "cores": 1, "kind": "reference",
-            "sample": f"{its} iterations of sk_solve (SK_LP_FIRST_ORDER, 1 thread, built from the reference's "
-                      f"c/src without OpenMP) on the same instance, {secs:.2f} s of loop time"}
+    gbs, secs, its = reference_loop_gbs(inst, iters, core)
+    return {"value": round(gbs, 4), "unit": "GB/s", "cores": core[1], "kind": "reference",
+            "sample": f"{its} iterations of sk_solve (SK_LP_FIRST_ORDER, {_core_text(core)}) on the same "
+                      f"instance, {secs:.2f} s of loop time"}
 
 
 def time_to_kkt(E, A, inst, eps=1e-6, limit_s=90.0):
@@ -228,11 +251,12 @@ def run_reference(args, world, rank):
     inst = I.lp_config1(SEED)
     nnz = int(inst["ptr"][-1])
     per_step = 2  # iterations of the reference loop per step: bounded sample of the workload
+    core = reference_core()
     for _ in range(args.warmup):
-        reference_loop_gbs(inst, 1)
+        reference_loop_gbs(inst, 1, core)
     total_secs, total_iters = 0.0, 0
     for _ in range(args.steps):
-        gbs, secs, its = reference_loop_gbs(inst, per_step)
+        gbs, secs, its = reference_loop_gbs(inst, per_step, core)
         total_secs += secs
         total_iters += its
     value = iteration_bytes(M if inst["m"] == M else inst["m"], inst["n"], nnz) * total_iters / total_secs / 1e9
@@ -241,8 +265,9 @@ def run_reference(args, world, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "m": inst["m"], "n": inst["n"], "nnz": nnz,
                        "iterations_per_step": per_step, "seed": SEED},
-            "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": 1, "kind": "reference",
-                             "sample": f"{per_step} iterations of the reference sk_solve first-order loop per step"},
+            "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": core[1], "kind": "reference",
+                             "sample": f"{per_step} iterations of the reference sk_solve first-order loop per step "
+                                       f"({_core_text(core)})"},
             "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0

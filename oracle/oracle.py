@@ -5,6 +5,7 @@ cpu_baseline / reference legs of bench.py; the product never imports it.
 
   liboracle.so                  C restatement of the reference path (pdhg_oracle.c)
   _ref/libsankhya_ref.so        the reference's own C core (sk_solve, sk_verify, ...)
+  _ref/libsankhya_ref_omp.so    the same core built with OpenMP (same bits, threaded csc_tmv)
   _ref/libsankhya_cuda_ref.so   the reference's CUDA prototype built for sm_100a
 """
 from __future__ import annotations
@@ -37,6 +38,7 @@ def load(name: str) -> C.CDLL:
     if name not in _libs:
         path = {"oracle": os.path.join(HERE, "liboracle.so"),
                 "ref": os.path.join(HERE, "_ref", "libsankhya_ref.so"),
+                "ref_omp": os.path.join(HERE, "_ref", "libsankhya_ref_omp.so"),
                 "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so")}[name]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")
@@ -306,8 +308,8 @@ def build_sk_model(keep: _Keep, inst, quadratic=False):
 
 
 def ref_options(primal_tol=1e-7, dual_tol=1e-7, iteration_limit=0, time_limit=0.0,
-                lp_engine=SK_LP_FIRST_ORDER, threads=1):
-    lib = load("ref")
+                lp_engine=SK_LP_FIRST_ORDER, threads=1, lib_name="ref"):
+    lib = load(lib_name)
     o = SkOptions()
     lib.sk_options_default(C.byref(o))
     o.primal_tol, o.dual_tol = primal_tol, dual_tol
@@ -316,12 +318,13 @@ def ref_options(primal_tol=1e-7, dual_tol=1e-7, iteration_limit=0, time_limit=0.
     return o
 
 
-def ref_sk_solve(inst, quadratic=False, **opts):
-    """Runs the reference's sk_solve; returns (status, dict with x, y, rowact, fields)."""
-    lib = load("ref")
+def ref_sk_solve(inst, quadratic=False, lib_name="ref", **opts):
+    """Runs the reference's sk_solve; returns (status, dict with x, y, rowact, fields).
+    lib_name "ref_omp" runs the OpenMP build (give `threads`)."""
+    lib = load(lib_name)
     keep = _Keep()
     model = build_sk_model(keep, inst, quadratic)
-    o = ref_options(**opts)
+    o = ref_options(lib_name=lib_name, **opts)
     s = SkSolution()
     lib.sk_solution_init(C.byref(s))
     st = lib.sk_solve(C.byref(model), C.byref(o), C.byref(s))

@@ -96,3 +96,14 @@ def test_clock_summary_parses_nvidia_smi_rows():
     empty = b.ClockSampler(0)
     empty.out = ""
     assert empty.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+
+def test_reference_core_prefers_the_openmp_build():
+    b = _bench()
+    lib_name, threads = b.reference_core()
+    omp = os.path.join(ROOT, "oracle", "_ref", "libsankhya_ref_omp.so")
+    if os.path.exists(omp):
+        assert lib_name == "ref_omp" and threads == len(os.sched_getaffinity(0))
+    else:
+        assert (lib_name, threads) == ("ref", 1)
+    assert "OpenMP" in b._core_text(("ref_omp", 8)) and "1 thread" in b._core_text(("ref", 1))

@@ -173,3 +173,19 @@ def test_oracle_live_against_reference_core(oracle, instances):
         assert np.array_equal(x, ref["x"]) and np.array_equal(y, ref["y"]) and np.array_equal(act, ref["rowact"])
     st, v = oracle.ref_sk_verify(inst, x, y)
     assert v == oracle.sk_verify(inst, x, y)
+
+
+def test_openmp_build_of_the_reference_core_gives_the_same_bits(oracle, instances):
+    """The OpenMP build (the timed CPU legs' core) splits only csc_tmv over columns, each
+    column's sum still in stored order: its sk_solve iterates equal the serial build's."""
+    import os
+    if not os.path.exists(os.path.join(os.path.dirname(oracle.__file__), "_ref", "libsankhya_ref_omp.so")):
+        pytest.skip("OpenMP build of the reference core absent")
+    inst = instances.lp_powerlaw(3, 20000, 40000, 400000)    # above csc_tmv's threading threshold
+    st0, ser = oracle.ref_sk_solve(inst, primal_tol=1e-300, dual_tol=1e-300, iteration_limit=60)
+    for threads in (1, 4, 8):
+        st, par = oracle.ref_sk_solve(inst, lib_name="ref_omp", threads=threads, primal_tol=1e-300, dual_tol=1e-300,
+                                      iteration_limit=60)
+        assert st == st0 == 0 and par["iterations"] == ser["iterations"] == 60
+        for k in ("x", "y", "rowact"):
+            assert np.array_equal(par[k], ser[k]), (threads, k)
