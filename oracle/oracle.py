@@ -6,6 +6,7 @@ cpu_baseline / reference legs of bench.py; the product never imports it.
   liboracle.so                  C restatement of the reference path (pdhg_oracle.c)
   _ref/libsankhya_ref.so        the reference's own C core (sk_solve, sk_verify, ...)
   _ref/libsankhya_ref_omp.so    the same core built with OpenMP (same bits, threaded csc_tmv)
+  _ref/libsihps_scaling_ref.so  the reference C++ core's Ruiz / Pock-Chambolle (src/lp/Scaling.cpp)
   _ref/libsankhya_cuda_ref.so   the reference's CUDA prototype built for sm_100a
 """
 from __future__ import annotations
@@ -39,6 +40,7 @@ def load(name: str) -> C.CDLL:
         path = {"oracle": os.path.join(HERE, "liboracle.so"),
                 "ref": os.path.join(HERE, "_ref", "libsankhya_ref.so"),
                 "ref_omp": os.path.join(HERE, "_ref", "libsankhya_ref_omp.so"),
+                "ref_scaling": os.path.join(HERE, "_ref", "libsihps_scaling_ref.so"),
                 "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so")}[name]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")
@@ -229,6 +231,30 @@ def pock_chambolle(inst, alpha=1.0):
     r, c = np.zeros(inst["m"]), np.zeros(inst["n"])
     lib.orc_pock_chambolle(C.byref(a), C.c_double(alpha), _p(r), _p(c))
     return r, c
+
+
+def _ref_scaling_call(name, inst, *args):
+    lib = load("ref_scaling")
+    keep = _Keep()
+    ptr, idx, val = keep.i(inst["ptr"]), keep.i(inst["idx"]), keep.d(inst["val"])
+    r, c = np.zeros(inst["m"]), np.zeros(inst["n"])
+    fn = getattr(lib, name)
+    fn.restype = C.c_int
+    rc = fn(C.c_int(inst["m"]), C.c_int(inst["n"]), C.c_int(int(inst["ptr"][-1])), _p(ptr, iptr), _p(idx, iptr),
+            _p(val), *args, _p(r), _p(c))
+    if rc != 0:
+        raise ValueError(f"{name} rejected the matrix")
+    return r, c
+
+
+def ref_ruiz(inst, max_iters=100, tol=1e-2):
+    """The reference's compute_ruiz_scaling (src/lp/Scaling.cpp): (row_scale, col_scale)."""
+    return _ref_scaling_call("ref_ruiz_scaling", inst, C.c_int(max_iters), C.c_double(tol))
+
+
+def ref_pock_chambolle(inst, alpha=1.0):
+    """The reference's compute_pock_chambolle_scaling (src/lp/Scaling.cpp)."""
+    return _ref_scaling_call("ref_pock_chambolle_scaling", inst, C.c_double(alpha))
 
 
 def pow2_scale(inst, passes=4):

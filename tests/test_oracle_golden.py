@@ -189,3 +189,27 @@ def test_openmp_build_of_the_reference_core_gives_the_same_bits(oracle, instance
         assert st == st0 == 0 and par["iterations"] == ser["iterations"] == 60
         for k in ("x", "y", "rowact"):
             assert np.array_equal(par[k], ser[k]), (threads, k)
+
+
+@pytest.mark.parametrize("name", ["lp60", "powerlaw20k", "config0"])
+def test_scaling_restatements_match_the_reference_cpp_core(oracle, instances, name):
+    """The oracle's Ruiz and Pock-Chambolle factors equal, bit for bit, those of the
+    reference C++ core's own compute_ruiz_scaling / compute_pock_chambolle_scaling
+    (src/lp/Scaling.cpp, compiled into oracle/_ref), including a Ruiz run that does not
+    reach its tolerance (the reference then falls back to the identity)."""
+    import os
+    if not os.path.exists(os.path.join(os.path.dirname(oracle.__file__), "_ref", "libsihps_scaling_ref.so")):
+        pytest.skip("reference scaling checker not built (make -C oracle ref)")
+    inst = {"lp60": lambda: instances.lp_uniform(12, 60, 150, 4),
+            "powerlaw20k": lambda: instances.lp_powerlaw(3, 20000, 40000, 400000),
+            "config0": lambda: instances.lp_config0(0)}[name]()
+    for max_iters, tol in ((100, 1e-2), (2, 1e-12)):
+        r0, c0, conv = oracle.ruiz(inst, max_iters, tol)
+        r1, c1 = oracle.ref_ruiz(inst, max_iters, tol)
+        assert np.array_equal(r0, r1) and np.array_equal(c0, c1), (max_iters, tol)
+        if not conv:
+            assert np.all(r1 == 1.0) and np.all(c1 == 1.0)
+    for alpha in (1.0, 0.5):
+        p0, q0 = oracle.pock_chambolle(inst, alpha)
+        p1, q1 = oracle.ref_pock_chambolle(inst, alpha)
+        assert np.array_equal(p0, p1) and np.array_equal(q0, q1), alpha
