@@ -7,6 +7,7 @@ cpu_baseline / reference legs of bench.py; the product never imports it.
   _ref/libsankhya_ref.so        the reference's own C core (sk_solve, sk_verify, ...)
   _ref/libsankhya_ref_omp.so    the same core built with OpenMP (same bits, threaded csc_tmv)
   _ref/libsihps_scaling_ref.so  the reference C++ core's Ruiz / Pock-Chambolle (src/lp/Scaling.cpp)
+  _ref/libsihps_pdlp_ref.so     the reference C++ core's GPU PDLP (src/cuda/GpuPdlp.cpp), needs a GPU
   _ref/libsankhya_cuda_ref.so   the reference's CUDA prototype built for sm_100a
 """
 from __future__ import annotations
@@ -41,6 +42,7 @@ def load(name: str) -> C.CDLL:
                 "ref": os.path.join(HERE, "_ref", "libsankhya_ref.so"),
                 "ref_omp": os.path.join(HERE, "_ref", "libsankhya_ref_omp.so"),
                 "ref_scaling": os.path.join(HERE, "_ref", "libsihps_scaling_ref.so"),
+                "ref_pdlp": os.path.join(HERE, "_ref", "libsihps_pdlp_ref.so"),
                 "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so")}[name]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")
@@ -255,6 +257,42 @@ def ref_ruiz(inst, max_iters=100, tol=1e-2):
 def ref_pock_chambolle(inst, alpha=1.0):
     """The reference's compute_pock_chambolle_scaling (src/lp/Scaling.cpp)."""
     return _ref_scaling_call("ref_pock_chambolle_scaling", inst, C.c_double(alpha))
+
+
+class RefPdlpParams(C.Structure):
+    """RefPdlpParams of ref_pdlp_shim.cpp (the reference's PdlpParams, plus `scale`)."""
+    _fields_ = [("eps_optimal", C.c_double), ("max_iterations", C.c_int), ("restart_period", C.c_int),
+                ("time_limit_seconds", C.c_double), ("power_iterations", C.c_int), ("adaptive_step", C.c_int),
+                ("eta_min_factor", C.c_double), ("eta_max_factor", C.c_double), ("scale", C.c_int),
+                ("reserved", C.c_int)]
+
+
+class RefPdlpStats(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("restarts", C.c_int),
+                ("rejected_steps", C.c_int), ("host_syncs", C.c_int), ("reserved", C.c_int),
+                ("primal_objective", C.c_double), ("dual_objective", C.c_double),
+                ("relative_primal_residual", C.c_double), ("relative_dual_residual", C.c_double),
+                ("relative_gap", C.c_double), ("matrix_norm", C.c_double), ("seconds", C.c_double)]
+
+
+def ref_gpupdlp(inst, eps=1e-8, max_iterations=500000, restart_period=64, power_iterations=30, adaptive=True,
+                eta_min_factor=1e-6, eta_max_factor=1e4, time_limit=0.0, scale=True):
+    """The reference's own GPU PDLP (GpuPdlp, with run_first_order's scaling when `scale`)
+    on the current CUDA device: (x, stats dict). Needs a GPU."""
+    lib = load("ref_pdlp")
+    keep = _Keep()
+    p = RefPdlpParams(eps, max_iterations, restart_period, time_limit, power_iterations, int(adaptive),
+                      eta_min_factor, eta_max_factor, int(scale), 0)
+    st = RefPdlpStats()
+    x = np.zeros(inst["n"])
+    fn = lib.ref_gpupdlp_solve
+    fn.restype = C.c_int
+    rc = fn(C.c_int(inst["m"]), C.c_int(inst["n"]), C.c_int(int(inst["ptr"][-1])), _p(keep.i(inst["ptr"]), iptr),
+            _p(keep.i(inst["idx"]), iptr), _p(keep.d(inst["val"])), _p(keep.d(inst["c"])), _p(keep.d(inst["cl"])),
+            _p(keep.d(inst["cu"])), _p(keep.d(inst["rl"])), _p(keep.d(inst["ru"])), C.byref(p), _p(x), C.byref(st))
+    if rc != 0:
+        raise RuntimeError("reference GpuPdlp failed")
+    return x, {k: getattr(st, k) for k, _ in RefPdlpStats._fields_}
 
 
 def pow2_scale(inst, passes=4):

@@ -213,3 +213,18 @@ def test_scaling_restatements_match_the_reference_cpp_core(oracle, instances, na
         p0, q0 = oracle.pock_chambolle(inst, alpha)
         p1, q1 = oracle.ref_pock_chambolle(inst, alpha)
         assert np.array_equal(p0, p1) and np.array_equal(q0, q1), alpha
+
+
+def test_reference_gpu_pdlp_checker_loads_and_fails_cleanly_without_a_device(oracle, instances):
+    """The reference C++ core's GPU PDLP (GpuPdlp, oracle/_ref/libsihps_pdlp_ref.so) is
+    built from the reference tree for comparisons on a B200. Here it must load and, with
+    no device, report failure through its C entry point instead of crashing."""
+    import os
+    import torch
+    if not os.path.exists(os.path.join(os.path.dirname(oracle.__file__), "_ref", "libsihps_pdlp_ref.so")):
+        pytest.skip("reference GPU PDLP checker not built (make -C oracle ref)")
+    oracle.load("ref_pdlp")
+    if torch.cuda.is_available():
+        return
+    with pytest.raises(RuntimeError):
+        oracle.ref_gpupdlp(instances.lp_uniform(12, 60, 150, 4), eps=1e-6)
