@@ -1,0 +1,42 @@
+"""The engine's PDLP against the reference C++ core's own GPU PDLP (GpuPdlp, with the
+scaling of run_first_order, src/lp/LpSolver.cpp:62-99), both on the same B200, on
+seeded instances: both must converge to 1e-6 relative KKT and agree on the objective;
+iterations and seconds are printed side by side.
+
+Run on demand with `python -m pytest tests/compare_reference_pdlp.py -s`: the file name
+keeps it out of the default collection until it has run on a B200 (it needs
+oracle/_ref/libsihps_pdlp_ref.so, built by `make -C oracle ref` where the reference
+sources are)."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+EPS = 1e-6
+
+CASES = {
+    "lp_uniform 300x700": lambda I: I.lp_uniform(11, 300, 700, 5),
+    "lp_uniform 20k x 40k": lambda I: I.lp_uniform(7, 20000, 40000, 5),
+    "lp_powerlaw 20k x 40k, 400k nnz": lambda I: I.lp_powerlaw(3, 20000, 40000, 400000),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_engine_pdlp_matches_reference_gpu_pdlp(engine, oracle, instances, name):
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libsihps_pdlp_ref.so")):
+        pytest.skip("reference GPU PDLP not built")
+    inst = CASES[name](instances)
+    A = engine.Matrix.from_instance(inst)
+    s = engine.pdlp_default_settings()
+    s.eps_optimal = EPS
+    rc, x, y, r = engine.pdlp_solve(A, inst, s)
+    A.close()
+    assert rc == 0 and r["status"] == 0, r
+    xr, st = oracle.ref_gpupdlp(inst, eps=EPS, scale=True)
+    assert st["converged"] == 1, st
+    obj, obj_ref = float(np.dot(inst["c"], x)), float(np.dot(inst["c"], xr))
+    assert abs(obj - obj_ref) <= 1e-5 * (1.0 + abs(obj_ref)), (obj, obj_ref)
+    print(f"\n{name}: engine {r['iterations']} it {r['seconds']:.3f} s | reference GpuPdlp "
+          f"{st['iterations']} it {st['seconds']:.3f} s | objective {obj:.10g} vs {obj_ref:.10g}")
