@@ -72,3 +72,24 @@ def test_learned_host_helpers(learned):
     assert np.isclose(learned.dual_scale(data), np.sqrt((9 + 16 + 0 + 0 + 1 + 1) / 6))
     assert learned.learned_weight(data) == 4.0
     assert learned.dual_scale([(None, None, np.zeros(4), 1.0)]) == 1e-12
+
+
+def test_qp_recipe(instances):
+    """The convex QP recipe (config 2 at a small size): A with a_per_col entries per
+    column, Q = D + L L^T full symmetric CSR and positive semidefinite, D log-uniform in
+    [1e-2, 1e2], boxes [-5, 5], rows feasible at x0."""
+    inst = instances.qp_diag_plus_lowrank(9, 300, 600, a_per_col=10, l_per_col=3)
+    _csr_ok(inst)
+    assert np.array_equal(np.bincount(inst["idx"], minlength=600), np.full(600, 10))
+    n = inst["n"]
+    Q = np.zeros((n, n))
+    for i in range(n):
+        Q[i, inst["q_idx"][inst["q_ptr"][i]:inst["q_ptr"][i + 1]]] = inst["q_val"][inst["q_ptr"][i]:inst["q_ptr"][i + 1]]
+    assert np.allclose(Q, Q.T, rtol=0, atol=1e-14)
+    assert np.linalg.eigvalsh(Q).min() > 0                           # D > 0 makes it definite
+    d = inst["qdiag"]
+    assert d.min() >= 1e-2 and d.max() <= 1e2
+    assert np.all(np.diag(Q) >= d - 1e-12)                          # L L^T adds a non-negative diagonal
+    assert np.all(inst["cl"] == -5.0) and np.all(inst["cu"] == 5.0)
+    act = instances.csr_matvec(inst["ptr"], inst["idx"], inst["val"], inst["x0"])
+    assert np.all(inst["rl"] <= act) and np.all(act <= inst["ru"])
