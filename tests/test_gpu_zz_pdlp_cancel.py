@@ -1,6 +1,6 @@
 """PDLP cancellation: settings version 4's `cancel` callback, the counterpart of
-GpuPdlp's PdlpParams::cancel (src/cuda/GpuPdlp.hpp:62-67), which LpMethod::HYBRID
-uses to stop the loser of its simplex / PDLP race. The callback is called once per
+GpuPdlp's PdlpParams::cancel (src/cuda/GpuPdlp.hpp:62-67), a flag the caller sets to
+stop a running solve. The callback is called once per
 restart window, where the host synchronizes anyway, so a non-zero answer stops the
 solve after the window that is running, with status 3. A callback that answers zero
 changes nothing. (Named to run after the other gpu files and before the
