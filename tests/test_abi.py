@@ -127,6 +127,8 @@ def test_loop_hook_validates_the_model_before_device_work(engine, oracle, instan
         man = json.load(open(os.path.join(ROOT, "tests", "golden", "manifest.json")))
         for name, seed, m, n, per_col, limits in man["lp"]:
             assert call(instances.lp_uniform(seed, m, n, per_col)) == 7, name
+        for name, seed, m, n, limits in man["qp"]:
+            assert call(instances.qp_diag_plus_lowrank(seed, m, n, a_per_col=4, l_per_col=2), quadratic=True) == 7, name
         assert call(lp) == 7 and call(qp, quadratic=True) == 7
 
     def setp(k, v):
