@@ -240,3 +240,26 @@ def test_pdlp_settings_versions(engine, instances):
         rc = L.sankhya_b200_pdlp_solve(C.byref(fake), d(inst["c"]), d(inst["rl"]), d(inst["ru"]), d(inst["cl"]),
                                        d(inst["cu"]), C.byref(s), None, None, d(x), None, C.byref(res))
         assert rc == -1 and message in engine.last_error(), (version, engine.last_error())
+
+
+def test_headers_compile_as_c_and_cxx_and_every_symbol_links(tmp_path):
+    """include/*.h are usable from C (C99, -Wall -Werror) and from C++: a program that
+    takes the address of every declared function compiles both ways and links against
+    the library."""
+    import subprocess
+    names = declared_symbols()
+    body = ["#include \"sankhya_cuda.h\"", "#include \"sankhya_b200.h\"", "#include <stdio.h>",
+            "int main(void) {", "    const void* fns[] = {"]
+    body += [f"        (const void*)&{n}," for n in names]
+    body += ["    };", "    printf(\"%d\\n\", (int)(sizeof(fns) / sizeof(fns[0])));", "    return 0;", "}"]
+    lib = os.path.join(ROOT, "the-solver_b200", "lib")
+    for lang, compiler, std, ext in (("c", "gcc", "-std=c99", ".c"), ("c++", "g++", "-std=c++17", ".cpp")):
+        src = tmp_path / ("abi" + ext)
+        src.write_text("\n".join(body) + "\n")
+        exe = tmp_path / ("abi_" + lang.replace("+", "x"))
+        r = subprocess.run([compiler, std, "-Wall", "-Werror", "-Wno-pedantic", "-I" + os.path.join(ROOT, "include"),
+                            str(src), "-L" + lib, "-lsankhya_cuda", "-Wl,-rpath," + lib, "-o", str(exe)],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, (lang, r.stderr[-3000:])
+        out = subprocess.run([str(exe)], capture_output=True, text=True)
+        assert out.returncode == 0 and int(out.stdout) == len(names), (lang, out.stdout, out.stderr)
