@@ -107,3 +107,15 @@ def test_reference_core_prefers_the_openmp_build():
     else:
         assert (lib_name, threads) == ("ref", 1)
     assert "OpenMP" in b._core_text(("ref_omp", 8)) and "1 thread" in b._core_text(("ref", 1))
+
+
+def test_committed_traffic_figures_parse_as_the_bench_reads_them():
+    """bench.py fills roofline.traffic from profiles/traffic_lp_config1.txt (key=value
+    lines, # comments): both launches' figures are there and are integers of the size
+    of one launch's DRAM bytes."""
+    path = os.path.join(ROOT, "profiles", "traffic_lp_config1.txt")
+    figures = dict(line.strip().split("=", 1) for line in open(path)
+                   if "=" in line and not line.lstrip().startswith("#"))
+    for key in ("primal", "dual"):
+        v = int(figures[key])
+        assert 1e8 < v < 1e9, (key, v)
