@@ -8,6 +8,7 @@ cpu_baseline / reference legs of bench.py; the product never imports it.
   _ref/libsankhya_ref_omp.so    the same core built with OpenMP (same bits, threaded csc_tmv)
   _ref/libsihps_scaling_ref.so  the reference C++ core's Ruiz / Pock-Chambolle (src/lp/Scaling.cpp)
   _ref/libsihps_pdlp_ref.so     the reference C++ core's GPU PDLP (src/cuda/GpuPdlp.cpp), needs a GPU
+  _ref/libsankhya_ref_hooked.so the C core with INTEGRATION.md's sk_solve block, calling the engine
   _ref/libsankhya_cuda_ref.so   the reference's CUDA prototype built for sm_100a
 """
 from __future__ import annotations
@@ -43,6 +44,7 @@ def load(name: str) -> C.CDLL:
                 "ref_omp": os.path.join(HERE, "_ref", "libsankhya_ref_omp.so"),
                 "ref_scaling": os.path.join(HERE, "_ref", "libsihps_scaling_ref.so"),
                 "ref_pdlp": os.path.join(HERE, "_ref", "libsihps_pdlp_ref.so"),
+                "ref_hooked": os.path.join(HERE, "_ref", "libsankhya_ref_hooked.so"),
                 "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so")}[name]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")

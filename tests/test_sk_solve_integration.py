@@ -17,15 +17,14 @@ pinned against the reference's sk_solve fixtures in tests/test_gpu_parity.py.
 """
 import ctypes as C
 import os
-import re
 import subprocess
 
 import numpy as np
 import pytest
 
+import hooked_core as H   # oracle/hooked_core.py: applies the block, builds the core
+
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
-C_SOURCES = ("sankhya_model.c", "sankhya_lu.c", "sankhya_mps.c", "sankhya_verify.c", "sk_lu.c", "sk_core.c",
-             "sk_simplex.c", "sk_scale.c", "sk_milp.c")
 
 
 def _reference():
@@ -36,35 +35,9 @@ def _reference():
     return mod.REFERENCE
 
 
-def _snippet():
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    section = doc.split("## 2.")[1].split("## 3.")[0]
-    block = re.search(r"```c\n(.*?)```", section, re.S).group(1)
-    include, body = block.split("\n", 1)
-    assert include.startswith('#include "sankhya_b200.h"')
-    return body
-
-
-def _patched_source(text, body):
-    start = text.index("static sk_status solve_continuous(")
-    loop = text.index("\n    start = sk_wall_seconds();\n", start)
-    done = text.index("\n    performed_iterations = iteration > maximum_iterations", loop)
-    done_end = text.index("\n", done + 1)
-    out = text[:loop + 1] + body + text[loop + 1:done_end + 1] + "after_loop:;\n" + text[done_end + 1:]
-    return out.replace('#include "sankhya.h"\n', '#include "sankhya.h"\n#include "sankhya_b200.h"\n', 1)
-
-
 def _build_core(ref, out, lib_dir, lib_name):
     """The patched core as a shared library linked to lib<lib_name>.so in lib_dir."""
-    src = os.path.join(ref, "c", "src")
-    patched = _patched_source(open(os.path.join(src, "sk_solve.c")).read(), _snippet())
-    cmd = ["gcc", "-O3", "-DNDEBUG", "-std=gnu11", "-fPIC", "-shared", "-DSANKHYA_WITH_B200",
-           "-I" + os.path.join(ref, "c", "include"), "-I" + os.path.join(ROOT, "include"),
-           "-x", "c", "-", "-x", "none"] + [os.path.join(src, f) for f in C_SOURCES] + [
-           "-L" + lib_dir, "-l" + lib_name, "-Wl,-rpath," + lib_dir, "-o", out, "-lm"]
-    r = subprocess.run(cmd, input=patched, capture_output=True, text=True)
-    assert r.returncode == 0, r.stderr[-3000:]
-    return out
+    return H.build(ref, out, lib_dir, lib_name)
 
 
 @pytest.fixture(scope="module")
@@ -152,7 +125,7 @@ def test_snippet_anchors_exist_once():
     body = body[:body.index("\n}\n")]
     assert body.count("\n    start = sk_wall_seconds();\n") == 1
     assert body.count("\n    performed_iterations = iteration > maximum_iterations") == 1
-    patched = _patched_source(text, _snippet())
+    patched = H.patched_source(text, H.snippet())
     assert patched.count("goto after_loop;") == 1 and patched.count("after_loop:;") == 1
 
 
