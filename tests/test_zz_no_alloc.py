@@ -9,7 +9,7 @@ library, so a solve allocates nothing. These tests call it through the C ABI and
 check it against the allocating entry point, sankhya_cuda_lp_pdhg, on two calls
 in a row (the array keeps the previous call's contents, so the second call checks
 that everything that must start at zero is cleared). The file is named to be
-collected last."""
+collected after the rest of the suite; only the test_zzz_ files follow it."""
 import ctypes as C
 
 import numpy as np

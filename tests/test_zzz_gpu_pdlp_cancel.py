@@ -3,8 +3,8 @@ GpuPdlp's PdlpParams::cancel (src/cuda/GpuPdlp.hpp:62-67), a flag the caller set
 stop a running solve. The callback is called once per
 restart window, where the host synchronizes anyway, so a non-zero answer stops the
 solve after the window that is running, with status 3. A callback that answers zero
-changes nothing. (Named to run after the other gpu files and before the
-allocation-free entry point's file, which is collected last.)"""
+changes nothing. (Named to run after every other gpu file, the allocation-free entry
+point's included.)"""
 import ctypes as C
 
 import numpy as np

@@ -5,8 +5,8 @@ loop of solve_continuous to the engine's sankhya_b200_pdhg_loop, whose iterates 
 the reference's own loop; so sk_solve's answer through the patched core must equal,
 bit for bit, the unpatched core's (oracle/_ref/libsankhya_ref.so), and the engine's
 timing record for this thread must hold the hook's iteration count, which shows the
-hook, not the block's CPU fallback, produced it. (Named to run after the other gpu
-files and before the allocation-free entry point's file, which is collected last.)"""
+hook, not the block's CPU fallback, produced it. (Named to run after every other gpu
+file, the allocation-free entry point's included.)"""
 import os
 
 import numpy as np

@@ -5,8 +5,8 @@ handle), through this library's entry points: the device product, the device
 transpose product and the host-array product. The reference holds its GPU result to
 1e-9 absolute and relative against the CPU product; here every product must meet
 that, and every row of up to 32 entries (the owning-lane path) must equal the
-sequential sum in stored order bit for bit. (Named to run after the other gpu files
-and before the allocation-free entry point's file, which is collected last.)"""
+sequential sum in stored order bit for bit. (Named to run after every other gpu file, the
+allocation-free entry point's included.)"""
 import numpy as np
 import pytest
 
