@@ -324,9 +324,13 @@ SANKHYA_CUDA_API int sankhya_b200_gnn_train_step(
    library routine: the model (c, bounds) and the solution are device pointers the
    caller owns, and the scratch (iterate buffers, reduction partials) lives in a
    16 MiB array inside the library that every GPU loading the library holds until
-   the process exits. Limit: 4*cols + 2*rows plus about 9.5 Ki doubles of partials
-   must fit in 2 Mi doubles; larger problems are rejected with -1 and a message.
-   The matrix must come from sankhya_cuda_csr_create. The first call on a device
+   the process exits. Limit: 4*C + 2*R + 128*SMs + 64 doubles must fit in
+   2 Mi (2,097,152) doubles, with C = cols and R = rows each rounded up to a
+   multiple of 32 and SMs the device's multiprocessor count (148 on a B200, so the
+   reduction partials take 18,944 doubles there); larger problems are rejected
+   with -1 and a message. The matrix must come from sankhya_cuda_csr_create, with
+   its handle unchanged since, and that call's device must be current (-1
+   otherwise). The first call on a device
    looks up the array's device address (cudaGetSymbolAddress) and must come before
    any stream capture. All calls share the array and it keeps the last call's
    contents: calls that overlap on the GPU race. Work is queued on the legacy

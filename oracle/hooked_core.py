@@ -1,7 +1,7 @@
 """TEST INFRASTRUCTURE ONLY: the reference's C core with the sk_solve integration block
-applied, as INTEGRATION.md section 2 writes it.
+(include/integration/sk_solve_hook.inc) applied.
 
-The block is read from INTEGRATION.md and inserted into the reference's
+The block is read from include/integration/sk_solve_hook.inc and inserted into the reference's
 c/src/sk_solve.c before the first-order loop of solve_continuous (at
 `start = sk_wall_seconds();`), with the `after_loop:` label after the
 `performed_iterations` assignment. The patched file goes to gcc on standard input
@@ -16,7 +16,6 @@ from __future__ import annotations
 
 import argparse
 import os
-import re
 import subprocess
 import sys
 
@@ -26,15 +25,12 @@ C_SOURCES = ("sankhya_model.c", "sankhya_lu.c", "sankhya_mps.c", "sankhya_verify
              "sk_simplex.c", "sk_scale.c", "sk_milp.c")
 
 
+HOOK = os.path.join(ROOT, "include", "integration", "sk_solve_hook.inc")
+
+
 def snippet() -> str:
-    """The body of INTEGRATION.md section 2's C block (its include line dropped)."""
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    section = doc.split("## 2.")[1].split("## 3.")[0]
-    block = re.search(r"```c\n(.*?)```", section, re.S).group(1)
-    include, body = block.split("\n", 1)
-    if not include.startswith('#include "sankhya_b200.h"'):
-        raise ValueError("INTEGRATION.md section 2 block does not start with the header include")
-    return body
+    """The integration block as a maintainer pastes it into solve_continuous."""
+    return open(HOOK).read()
 
 
 def patched_source(text: str, body: str) -> str:

@@ -8,7 +8,7 @@ cpu_baseline / reference legs of bench.py; the product never imports it.
   _ref/libsankhya_ref_omp.so    the same core built with OpenMP (same bits, threaded csc_tmv)
   _ref/libsihps_scaling_ref.so  the reference C++ core's Ruiz / Pock-Chambolle (src/lp/Scaling.cpp)
   _ref/libsihps_pdlp_ref.so     the reference C++ core's GPU PDLP (src/cuda/GpuPdlp.cpp), needs a GPU
-  _ref/libsankhya_ref_hooked.so the C core with INTEGRATION.md's sk_solve block, calling the engine
+  _ref/libsankhya_ref_hooked.so the C core with include/integration/sk_solve_hook.inc applied, calling the engine
   _ref/libsankhya_cuda_ref.so   the reference's CUDA prototype built for sm_100a
 """
 from __future__ import annotations
@@ -382,6 +382,17 @@ def ref_options(primal_tol=1e-7, dual_tol=1e-7, iteration_limit=0, time_limit=0.
     o.iteration_limit, o.time_limit = iteration_limit, time_limit
     o.lp_engine, o.threads, o.verbosity = lp_engine, threads, 0
     return o
+
+
+def reference_tree():
+    """The reference checkout the checkers are built from, or None where it is absent:
+    $SANKHYA_REFERENCE, else the location oracle/Makefile builds from by default."""
+    import subprocess
+    path = os.environ.get("SANKHYA_REFERENCE")
+    if not path:
+        r = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True)
+        path = r.stdout.strip() if r.returncode == 0 else ""
+    return path if path and os.path.isfile(os.path.join(path, "c", "src", "sk_solve.c")) else None
 
 
 def ref_sk_solve(inst, quadratic=False, lib_name="ref", **opts):

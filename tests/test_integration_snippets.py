@@ -1,4 +1,4 @@
-"""The callers written in INTEGRATION.md section 3, compiled inside the reference
+"""The callers in include/integration/, compiled inside the reference
 translation units they belong to (from standard input; no copy of a source is
 written), so the names, types and signatures they use must match both the
 reference's code and this library's C ABI:
@@ -11,7 +11,6 @@ reference's code and this library's C ABI:
   c/src/sk_milp.c, where the `milp` driver struct it reads (M->m, M->lp_opt) is
   defined, checked with gcc -fsyntax-only."""
 import os
-import re
 import subprocess
 
 import pytest
@@ -20,25 +19,22 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 
 
 def _reference():
-    import importlib.util
-    spec = importlib.util.spec_from_file_location("graft_entry", os.path.join(ROOT, "__graft_entry__.py"))
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    return mod.REFERENCE
+    import oracle as O
+    ref = O.reference_tree()
+    if ref is None:
+        pytest.skip("reference sources absent (set SANKHYA_REFERENCE)")
+    return ref
 
 
-def _section3():
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    return doc.split("## 3.")[1].split("## 4.")[0]
+INTEGRATION = os.path.join(ROOT, "include", "integration")
 
 
 def _block():
-    return re.search(r"```cpp\n(.*?)```", _section3(), re.S).group(1)
+    return open(os.path.join(INTEGRATION, "lpsolver_run_first_order.inc")).read()
 
 
 def _milp_block():
-    blocks = re.findall(r"```c\n(.*?)```", _section3(), re.S)
-    return [b for b in blocks if "sankhya_b200_shared_batch_pdhg(" in b][0]
+    return open(os.path.join(INTEGRATION, "sk_milp_batch.inc")).read()
 
 
 def _spliced(text, block):

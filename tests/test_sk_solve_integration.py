@@ -1,4 +1,4 @@
-"""The `sk_solve` integration written in INTEGRATION.md section 2, applied as written.
+"""The `sk_solve` integration (include/integration/sk_solve_hook.inc), applied as written.
 
 Where the reference sources are present, the test takes the reference's
 c/src/sk_solve.c, inserts the documented hook before the first-order loop of
@@ -28,11 +28,11 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 
 
 def _reference():
-    import importlib.util
-    spec = importlib.util.spec_from_file_location("graft_entry", os.path.join(ROOT, "__graft_entry__.py"))
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    return mod.REFERENCE
+    import oracle as O
+    ref = O.reference_tree()
+    if ref is None:
+        pytest.skip("reference sources absent (set SANKHYA_REFERENCE)")
+    return ref
 
 
 def _build_core(ref, out, lib_dir, lib_name):

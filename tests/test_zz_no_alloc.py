@@ -7,9 +7,11 @@ device-wide synchronisation cudaMalloc/cudaFree can impose on other streams. Thi
 and the solution and keeps its scratch in a fixed 16 MiB array inside the
 library, so a solve allocates nothing. These tests call it through the C ABI and
 check it against the allocating entry point, sankhya_cuda_lp_pdhg, on two calls
-in a row (the array keeps the previous call's contents, so the second call checks
-that everything that must start at zero is cleared). The file is named to be
-collected after the rest of the suite; only the test_zzz_ files follow it."""
+of the same instance with a solve of a different, larger instance between them:
+the array keeps the previous call's contents, so the second compared call starts
+on scratch that another problem left behind and checks that everything that must
+start at zero is cleared. The file is named to be collected after the rest of the
+suite; only the test_zzz_ files follow it."""
 import ctypes as C
 
 import numpy as np
@@ -32,24 +34,36 @@ def _device_model(inst):
     return {k: torch.tensor(np.asarray(inst[k], dtype=np.float64), device="cuda") for k in ("c", "rl", "ru", "cl", "cu")}
 
 
-def test_matches_allocating_entry_on_two_calls(engine, instances):
+def _solve(f, engine, A, d, n, s):
     import torch
+    sol = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+    res = engine.Result()
+    rc = f(C.byref(A.handle), d["c"].data_ptr(), d["rl"].data_ptr(), d["ru"].data_ptr(), d["cl"].data_ptr(),
+           d["cu"].data_ptr(), s, sol.data_ptr(), C.byref(res))
+    assert rc == 0, engine.last_error()
+    return sol.cpu().numpy(), res.as_dict()
+
+
+def test_matches_allocating_entry_on_two_calls(engine, instances):
     inst = instances.lp_uniform(41, 500, 1200, 5)
+    other = instances.lp_uniform(42, 3000, 7000, 5)   # larger: its scratch covers the first one's
     A = engine.Matrix.from_instance(inst)
+    B = engine.Matrix.from_instance(other)
     s = engine.settings(300, 50, 0.05, 0.05, 1.0, 1e-9)
     rc, x_ref, _, r_ref = engine.pdhg(A, inst, s)
     assert rc == 0
+    rc, xo_ref, _, ro_ref = engine.pdhg(B, other, s)
+    assert rc == 0
     f = _bind(engine)
-    d = _device_model(inst)
+    d, do = _device_model(inst), _device_model(other)
     for call in range(2):
-        sol = torch.full((inst["n"],), float("nan"), dtype=torch.float64, device="cuda")
-        res = engine.Result()
-        rc = f(C.byref(A.handle), d["c"].data_ptr(), d["rl"].data_ptr(), d["ru"].data_ptr(), d["cl"].data_ptr(),
-               d["cu"].data_ptr(), s, sol.data_ptr(), C.byref(res))
-        assert rc == 0, engine.last_error()
+        x, r = _solve(f, engine, A, d, inst["n"], s)
         # same kernels in the same order: bit-identical to the allocating entry point
-        assert np.array_equal(sol.cpu().numpy(), x_ref), call
-        assert res.as_dict() == r_ref, call
+        assert np.array_equal(x, x_ref), call
+        assert r == r_ref, call
+        if call == 0:
+            xo, ro = _solve(f, engine, B, do, other["n"], s)
+            assert np.array_equal(xo, xo_ref) and ro == ro_ref
 
 
 def test_converges_like_the_allocating_entry(engine, instances):
@@ -66,6 +80,23 @@ def test_converges_like_the_allocating_entry(engine, instances):
              d["cu"].data_ptr(), s, sol.data_ptr(), C.byref(res)) == 0
     assert res.status == 0 and res.iterations == r_ref["iterations"]
     assert abs(sol.item() - 1.0) <= 1e-3
+
+
+def test_rejects_a_handle_pointing_at_other_arrays(engine, instances):
+    """A copy of a handle whose values pointer was moved is not the planned matrix."""
+    import torch
+    inst = instances.lp_uniform(43, 50, 120, 4)
+    A = engine.Matrix.from_instance(inst)
+    other_values = torch.tensor(inst["val"] * 2.0, device="cuda")
+    h = engine.CSR(A.handle.rows, A.handle.cols, A.handle.nnz, A.handle.device_row_offsets,
+                   A.handle.device_column_indices, other_values.data_ptr())
+    f = _bind(engine)
+    d = _device_model(inst)
+    sol = torch.zeros(inst["n"], dtype=torch.float64, device="cuda")
+    res = engine.Result()
+    rc = f(C.byref(h), d["c"].data_ptr(), d["rl"].data_ptr(), d["ru"].data_ptr(), d["cl"].data_ptr(),
+           d["cu"].data_ptr(), engine.settings(10, 5, 0.1, 0.1, 1.0, 1e-6), sol.data_ptr(), C.byref(res))
+    assert rc == -1 and "sankhya_cuda_csr_create" in engine.last_error()
 
 
 def test_rejects_sizes_beyond_the_scratch(engine):

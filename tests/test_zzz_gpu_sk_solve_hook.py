@@ -1,5 +1,5 @@
-"""sk_solve through the reference's C core with the integration block of INTEGRATION.md
-section 2 applied (oracle/_ref/libsankhya_ref_hooked.so, built by oracle/hooked_core.py
+"""sk_solve through the reference's C core with the integration block
+include/integration/sk_solve_hook.inc applied (oracle/_ref/libsankhya_ref_hooked.so, built by oracle/hooked_core.py
 where the reference sources are present). On a GPU the block hands the first-order
 loop of solve_continuous to the engine's sankhya_b200_pdhg_loop, whose iterates equal
 the reference's own loop; so sk_solve's answer through the patched core must equal,

@@ -69,7 +69,6 @@ Plan::~Plan() {
     cudaFree(d_at_idx);
     cudaFree(d_at_val);
     cudaFree(d_tile_at);
-    cudaFree(d_err);
     cudaFree(d_a_idx);
     cudaFree(d_a_val);
     solve_cache.reset();
@@ -89,6 +88,8 @@ int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const
               std::shared_ptr<Plan>* out) {
     auto plan = std::make_shared<Plan>();
     cudaGetDevice(&plan->device);
+    plan->src_idx = m->device_column_indices;
+    plan->src_val = m->device_values;
     const int rows = m->rows, cols = m->cols, nnz = m->nnz;
 
     std::vector<int> tiles_a = build_tiles(rows, h_ptr);
@@ -112,8 +113,6 @@ int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const
     if (upload(reinterpret_cast<void**>(&plan->d_tile_a), tiles_a.data(), tiles_a.size() * sizeof(int), "cudaMalloc tiles(A)") ||
         upload(reinterpret_cast<void**>(&plan->d_tile_at), tiles_at.data(), tiles_at.size() * sizeof(int), "cudaMalloc tiles(A^T)"))
         return -1;
-    B200_TRY(cudaMalloc(reinterpret_cast<void**>(&plan->d_err), sizeof(unsigned int)), "cudaMalloc error word");
-    B200_TRY(cudaMemset(plan->d_err, 0, sizeof(unsigned int)), "clear error word");
     const int* a_idx = static_cast<const int*>(m->device_column_indices);
     const double* a_val = static_cast<const double*>(m->device_values);
     if ((reinterpret_cast<uintptr_t>(a_idx) | reinterpret_cast<uintptr_t>(a_val)) & 15u) {
@@ -132,7 +131,6 @@ int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const
     plan->a.val = a_val;
     plan->a.ntiles = static_cast<int>(tiles_a.size()) / 2 - 1;
     plan->a.tile = reinterpret_cast<const int2*>(plan->d_tile_a);
-    plan->a.err = plan->d_err;
     plan->at.rows = cols;
     plan->at.cols = rows;
     plan->at.nnz = nnz;
@@ -141,7 +139,6 @@ int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const
     plan->at.val = plan->d_at_val;
     plan->at.ntiles = static_cast<int>(tiles_at.size()) / 2 - 1;
     plan->at.tile = reinterpret_cast<const int2*>(plan->d_tile_at);
-    plan->at.err = plan->d_err;
     *out = std::move(plan);
     return 0;
 }
@@ -170,28 +167,45 @@ void unregister_plan(const void* key) {
     }
 }
 
-bool find_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out) {
-    if (m == nullptr) return false;
+// The registered plan of m when it describes the same arrays (offsets, indices,
+// values and sizes), else null.
+static std::shared_ptr<Plan> registered(const SankhyaCudaCSR* m) {
     std::lock_guard<std::mutex> lock(g_registry_mutex);
     auto it = registry().find(m->device_row_offsets);
-    if (it == registry().end() || it->second->a.rows != m->rows || it->second->a.cols != m->cols ||
-        it->second->a.nnz != m->nnz)
-        return false;
-    *out = it->second;
-    return true;
+    if (it == registry().end()) return nullptr;
+    const Plan& p = *it->second;
+    if (p.a.rows != m->rows || p.a.cols != m->cols || p.a.nnz != m->nnz || p.src_idx != m->device_column_indices ||
+        p.src_val != m->device_values)
+        return nullptr;
+    return it->second;
+}
+
+// A plan's arrays are memory of the device that was current when it was made.
+static int check_device(const Plan& plan) {
+    int current = -1;
+    B200_TRY(cudaGetDevice(&current), "cudaGetDevice");
+    if (current == plan.device) return 0;
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "the matrix was created on device %d but device %d is current", plan.device,
+                  current);
+    return fail_msg(msg);
+}
+
+int find_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out) {
+    if (m == nullptr) return fail_msg("null device CSR pointer");
+    std::shared_ptr<Plan> p = registered(m);
+    if (!p) return fail_msg("this entry point needs a matrix made by sankhya_cuda_csr_create and not changed since");
+    if (check_device(*p)) return -1;
+    *out = std::move(p);
+    return 0;
 }
 
 int get_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out) {
     if (m == nullptr) return fail_msg("null device CSR pointer");
-    {
-        std::lock_guard<std::mutex> lock(g_registry_mutex);
-        auto it = registry().find(m->device_row_offsets);
-        if (it != registry().end() && it->second->a.rows == m->rows && it->second->a.cols == m->cols &&
-            it->second->a.nnz == m->nnz && (it->second->a.val == m->device_values || it->second->d_a_val) &&
-            (it->second->a.idx == m->device_column_indices || it->second->d_a_idx)) {
-            *out = it->second;
-            return 0;
-        }
+    if (std::shared_ptr<Plan> p = registered(m)) {
+        if (check_device(*p)) return -1;
+        *out = std::move(p);
+        return 0;
     }
     // A handle filled by the caller: bring its CSR back once and plan it.
     if (m->rows < 0 || m->cols < 0 || m->nnz < 0) return fail_msg("invalid device CSR dimensions");

@@ -62,13 +62,12 @@ struct TileCsrT {
     const int* idx = nullptr;
     const T* val = nullptr;
     const int2* tile = nullptr;   // chunk boundaries: (first row, first nonzero)
-    unsigned int* err = nullptr;  // counts bounded device waits that gave up (may be null)
 
     template <class U>
     TileCsrT<U> with_values(const U* v) const {
         TileCsrT<U> o;
         o.rows = rows; o.cols = cols; o.nnz = nnz; o.ntiles = ntiles;
-        o.ptr = ptr; o.idx = idx; o.val = v; o.tile = tile; o.err = err;
+        o.ptr = ptr; o.idx = idx; o.val = v; o.tile = tile;
         return o;
     }
 };
@@ -84,9 +83,10 @@ struct Plan {
     int* d_at_idx = nullptr;
     double* d_at_val = nullptr;
     int* d_tile_at = nullptr;
-    unsigned int* d_err = nullptr;  // wait-timeout counter shared by this plan's launches
-    int* d_a_idx = nullptr;         // owned copies of A when the caller's arrays are
-    double* d_a_val = nullptr;      // not 16-byte aligned (TMA bulk copies need it)
+    int* d_a_idx = nullptr;         // owned copies of A when the caller's arrays are not
+    double* d_a_val = nullptr;      // 16-byte aligned (the bulk L2 prefetch of a chunk needs it)
+    const void* src_idx = nullptr;  // the handle's device_column_indices / device_values at
+    const void* src_val = nullptr;  // planning time: a handle pointing elsewhere is another matrix
     double row_mass_max = 0.0;   // filled lazily by users that need it
     std::mutex workspace_mutex;   // held by the solve that uses `solve_cache`
     std::shared_ptr<void> solve_cache; // workspace + captured graphs of the last fixed-step solve
@@ -100,9 +100,13 @@ int make_plan(const SankhyaCudaCSR* m, const int* h_ptr, const int* h_idx, const
 
 // Registered plan of a handle made by sankhya_cuda_csr_create, else a plan
 // built now from the handle's device arrays (copied back to the host once).
+// Fails (-1) when the plan lives on another device than the current one: its
+// arrays are that device's memory.
 int get_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out);
-// Registered plan only (never builds one, never allocates); false if absent.
-bool find_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out);
+// Registered plan only (never builds one, never allocates): -1 with a message
+// when the handle has none, points at other arrays than the planned ones, or the
+// plan lives on another device than the current one.
+int find_plan(const SankhyaCudaCSR* m, std::shared_ptr<Plan>* out);
 void register_plan(const void* key, std::shared_ptr<Plan> plan);
 void unregister_plan(const void* key);
 

@@ -81,11 +81,10 @@ extern "C" int sankhya_b200_lp_pdhg_device_noalloc(const SankhyaCudaCSR* matrix,
         s.time_limit < 0.0 || s.tau <= 0.0 || s.sigma <= 0.0)
         return fail_msg("invalid PDHG settings");
     std::shared_ptr<Plan> plan;
-    if (!find_plan(matrix, &plan))
-        return fail_msg("the allocation-free entry point needs a matrix made by sankhya_cuda_csr_create");
+    if (find_plan(matrix, &plan)) return -1;  // also rejects a matrix made on another device
     const int rows = matrix->rows, cols = matrix->cols;
-    int device = 0, sms = 148;
-    cudaGetDevice(&device);
+    const int device = plan->device;
+    int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     // scratch layout (doubles): x[2], x_bar, x_prev (cols each), y[2] (rows each),
     // two reduction-partial areas, 32 result slots and one flag word

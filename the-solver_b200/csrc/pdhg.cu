@@ -225,15 +225,6 @@ struct Workspace {
     }
 };
 
-// True when a bounded device wait of this plan's launches gave up (the word is
-// then cleared so the next call starts clean).
-static bool wait_timed_out(const Plan& plan) {
-    unsigned int word = 0;
-    if (!plan.d_err || cudaMemcpy(&word, plan.d_err, sizeof(word), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
-    if (word) cudaMemset(plan.d_err, 0, sizeof(word));
-    return word != 0;
-}
-
 // A host-visible pinned slot for checkpoint results, one per thread.
 static double* pinned_out() {
     struct Holder {
@@ -558,7 +549,6 @@ static int solve_fixed(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessi
         B200_TRY(cudaStreamSynchronize(stream), "checkpoint");
         ts.last.checkpoint_ms += t_chk.stop();
         ts.last.checkpoints += 1;
-        if (wait_timed_out(*plan)) return fail_msg("device wait for a tile copy gave up");
         const double nonfinite = std::max(host[0], host[8]);
         const double objective = host[9];
         if (nonfinite > 0.0 || !std::isfinite(objective)) {

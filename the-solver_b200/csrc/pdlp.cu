@@ -108,6 +108,34 @@ __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, T* __res
     }
 }
 
+// The adaptive step of Applegate et al., "Practical large-scale linear
+// programming using primal-dual hybrid gradient" (NeurIPS 2021, section 3.1).
+// For a trial move (dx, dy) made with step `used`, PDHG stays stable while the
+// step is at most  |dz|^2_w / (2 |dy' A dx|),  with |dz|^2_w = w |dx|^2 + |dy|^2 / w
+// (w the primal weight). The move is kept when `used` is within that limit. The
+// next step is min((1 - (k+1)^-0.3) limit, (1 + (k+1)^-0.6) used) for the k-th
+// trial: both factors tend to 1, so the step settles just under the limit.
+// With no interaction (or no movement) the limit is the largest allowed step;
+// a next step that is not a positive finite number keeps `used`; the result is
+// clamped to [lo, hi]. The operations, and so the rounding, follow the
+// reference's device code (src/cuda/PdlpKernels.cu:454-493).
+struct StepRule {
+    double limit, next;
+    bool keep;
+};
+__device__ __forceinline__ StepRule step_rule(double used, double w, double dx2, double dy2, double cross, double k,
+                                              double lo, double hi) {
+    StepRule r;
+    const double half_norm = 0.5 * (w * dx2 + dy2 / w);
+    r.limit = (cross > 0.0 && half_norm > 0.0) ? half_norm / cross : hi;
+    r.keep = used <= r.limit;
+    const double damp = 1.0 - pow(k + 1.0, -0.3), boost = 1.0 + pow(k + 1.0, -0.6);
+    double next = fmin(damp * r.limit, boost * used);
+    if (!(next > 0.0 && isfinite(next))) next = used;
+    r.next = fmin(fmax(next, lo), hi);
+    return r;
+}
+
 // K2 (PdlpKernels.cu:391-400 primal candidate + the |dx|^2 part of :405-430)
 template <class T>
 struct PrimalCandEpi {
@@ -187,26 +215,17 @@ struct ProbeEpi {
             __syncthreads();
         }
         if (threadIdx.x != 0) return;
-        const double dx_sq = red[0][0], dy_sq = red[1][0], inter = fabs(red[2][0]);
-        const double omega = st->omega;
-        const double movement = 0.5 * (omega * dx_sq + dy_sq / omega);
-        const double eta_used = st->eta;
-        const double eta_bar = (inter > 0.0 && movement > 0.0) ? movement / inter : st->eta_max;
-        const bool accept = eta_used <= eta_bar;
-        const double k = st->updates + 1.0;
-        const double shrink = 1.0 - pow(k + 1.0, -0.3);
-        const double grow = 1.0 + pow(k + 1.0, -0.6);
-        double eta_next = fmin(shrink * eta_bar, grow * eta_used);
-        if (!(eta_next > 0.0) || !isfinite(eta_next)) eta_next = eta_used;
-        eta_next = fmin(fmax(eta_next, st->eta_min), st->eta_max);
-        st->eta = eta_next;
-        st->eta_bar = eta_bar;
-        st->dx_sq = dx_sq;
-        st->dy_sq = dy_sq;
-        st->interaction = inter;
-        st->accepted = accept ? 1.0 : 0.0;
-        st->updates = k;
-        if (accept) st->accept_count += 1.0;
+        const double probe = st->updates + 1.0;
+        const StepRule rule = step_rule(st->eta, st->omega, red[0][0], red[1][0], fabs(red[2][0]), probe,
+                                        st->eta_min, st->eta_max);
+        st->dx_sq = red[0][0];
+        st->dy_sq = red[1][0];
+        st->interaction = fabs(red[2][0]);
+        st->eta_bar = rule.limit;
+        st->eta = rule.next;
+        st->updates = probe;
+        st->accepted = rule.keep ? 1.0 : 0.0;
+        st->accept_count += rule.keep ? 1.0 : 0.0;
         st->ticket = 0u;
     }
 };
@@ -1089,7 +1108,7 @@ struct Core {
     // and rises again, or after 0.36 of all iterations; at a restart the primal
     // weight moves halfway (in log) to |y+ - y0| / |x+ - x0|. Termination on the
     // relative KKT of T(z) at each window's end.
-    int run_halpern(const LoopParams& lp, LoopStats* out, const Plan* plan) {
+    int run_halpern(const LoopParams& lp, LoopStats* out) {
         const size_t nb = sizeof(T) * static_cast<size_t>(std::max(n, 1));
         const size_t mb = sizeof(T) * static_cast<size_t>(std::max(m, 1));
         for (T* v : {x_sum, x_cand, x_avg, aty}) cudaMemsetAsync(v, 0, nb, stream);
@@ -1115,13 +1134,6 @@ struct Core {
             if (halpern_window(period, slot)) return -1;
             B200_TRY(cudaStreamSynchronize(stream), "Halpern window");
             ++out->syncs;
-            if (plan && plan->d_err) {
-                unsigned int word = 0;
-                if (cudaMemcpy(&word, plan->d_err, sizeof(word), cudaMemcpyDeviceToHost) == cudaSuccess && word) {
-                    cudaMemset(plan->d_err, 0, sizeof(word));
-                    return fail_msg("device wait gave up");
-                }
-            }
             iteration += period;
             since_restart += period;
             const double* h = host;
@@ -1173,8 +1185,8 @@ struct Core {
 
     // Starting point already in x, y (T). Sets up A x, the restart reference
     // and the step state, then runs restarted windows (GpuPdlp.cpp:252-534).
-    int run(const LoopParams& lp, LoopStats* out, const Plan* plan) {
-        if (lp.halpern) return run_halpern(lp, out, plan);
+    int run(const LoopParams& lp, LoopStats* out) {
+        if (lp.halpern) return run_halpern(lp, out);
         const size_t nb = sizeof(T) * static_cast<size_t>(std::max(n, 1));
         const size_t mb = sizeof(T) * static_cast<size_t>(std::max(m, 1));
         for (T* v : {x_sum, x_cand, x_avg, aty}) cudaMemsetAsync(v, 0, nb, stream);
@@ -1218,13 +1230,6 @@ struct Core {
             if (window(period, lp.adaptive, tau, sigma, slot)) return -1;
             B200_TRY(cudaStreamSynchronize(stream), "PDLP window");
             ++out->syncs;
-            if (plan && plan->d_err) {
-                unsigned int word = 0;
-                if (cudaMemcpy(&word, plan->d_err, sizeof(word), cudaMemcpyDeviceToHost) == cudaSuccess && word) {
-                    cudaMemset(plan->d_err, 0, sizeof(word));
-                    return fail_msg("device wait gave up");
-                }
-            }
             iteration += period;
             iterations_since_restart += period;
             ++windows_since_restart;
@@ -1421,7 +1426,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         lp.max_iterations = s.max_iterations;
         lp.cost_norm = cost_norm;
         lp.bound_norm = bound_norm;
-        if (hi.run(lp, &stats, plan.get())) return -1;
+        if (hi.run(lp, &stats)) return -1;
         launches += hi.launches;
     } else {
         // -------------------------------------- FP32 iterations, then an FP64 finish
@@ -1460,7 +1465,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         flp.cost_norm = cost_norm;
         flp.bound_norm = bound_norm;
         LoopStats fs;
-        if (lo.run(flp, &fs, plan.get())) return -1;
+        if (lo.run(flp, &fs)) return -1;
         stats = fs;
         k_widen<<<gv, kThreads, 0, stream>>>(n, m, lo.x, lo.y, sc.cl, sc.cu, hi.x, hi.y);
         const long long left = s.max_iterations - fs.iterations;
@@ -1472,7 +1477,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
             lp.omega0 = fs.omega;
             lp.eta0 = fs.eta;
             LoopStats fin;
-            if (hi.run(lp, &fin, plan.get())) return -1;
+            if (hi.run(lp, &fin)) return -1;
             ++refinements;
             stats.iterations += fin.iterations;
             stats.restarts += fin.restarts;
