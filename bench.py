@@ -197,44 +197,153 @@ def _core_text(core):
             else "1 thread, the reference's c/src built without OpenMP")
 
 
-def cpu_baseline(inst, target_seconds=12.0):
-    """Bounded sample of the reference CPU PDHG on this instance (rank 0, N=1)."""
+# Iterations of the reference loop per sk_solve call in both CPU legs (the cpu_baseline
+# sample and each step of --impl reference). sk_solve's loop time includes one extra
+# product at the last iteration (its final checkpoint), so short calls understate the
+# loop's rate: at 64 iterations that extra product is under 1 % of the call.
+REFERENCE_ITERS_PER_CALL = 64
+
+
+def cpu_baseline(inst, calls=2):
+    """Bounded sample of the reference CPU PDHG on this instance (rank 0, N=1):
+    `calls` sk_solve calls of REFERENCE_ITERS_PER_CALL iterations after one
+    warm-up call of one iteration."""
     core = reference_core()
-    gbs1, secs1, it1 = reference_loop_gbs(inst, 1, core)
-    iters = int(max(2, min(200, target_seconds / max(secs1, 1e-3))))
-    gbs, secs, its = reference_loop_gbs(inst, iters, core)
+    reference_loop_gbs(inst, 1, core)
+    secs, its = 0.0, 0
+    for _ in range(calls):
+        _, s, i = reference_loop_gbs(inst, REFERENCE_ITERS_PER_CALL, core)
+        secs += s
+        its += i
+    nnz = int(inst["ptr"][-1])
+    gbs = iteration_bytes(inst["m"], inst["n"], nnz) * its / secs / 1e9
     return {"value": round(gbs, 4), "unit": "GB/s", "cores": core[1], "kind": "reference",
             "sample": f"{its} iterations of sk_solve (SK_LP_FIRST_ORDER, {_core_text(core)}) on the same "
                       f"instance, {secs:.2f} s of loop time"}
 
 
-def time_to_kkt(E, A, inst, eps=1e-6, limit_s=90.0):
-    """Wall time of sankhya_b200_pdlp_solve to eps relative KKT on the same instance:
-    plain FP64 PDLP (GpuPdlp's restarted adaptive loop) versus FP32 inner iterations
-    with an FP64 finish, and the reflected restarted Halpern loop in FP64 and with the
-    FP32 phase. Host arrays in and out, scaling included."""
-    out = {"eps": eps, "relative_kkt": "max(primal, dual, gap) as in GpuPdlp"}
-    runs = (("fp64", E.FP64, E.PDLP_ADAPTIVE), ("fp32_refined", E.FP32_REFINE, E.PDLP_ADAPTIVE),
-            ("halpern_fp64", E.FP64, E.PDLP_HALPERN), ("halpern_fp32_refined", E.FP32_REFINE, E.PDLP_HALPERN))
-    for name, prec, alg in runs:
-        s = E.pdlp_default_settings()
-        s.eps_optimal, s.precision, s.time_limit, s.max_iterations = eps, prec, limit_s, 2_000_000
-        s.algorithm = alg
+def _marginal_ms(call, reps=3):
+    """Wall-time cost of one more iteration: (best of reps at 200 iterations - best of
+    reps at 100) / 100; both calls pay the same setup, uploads, one checkpoint and the
+    download, which the difference cancels."""
+    best = {}
+    for its in (100, 200):
+        call(its)                                  # warm-up (allocations, graphs)
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            call(its)
+            ts.append(time.perf_counter() - t0)
+        best[its] = min(ts)
+    return 1e3 * (best[200] - best[100]) / 100.0
+
+
+def reference_gpu_baseline(E, A, inst, ps, ds, limit_s=120.0):
+    """The reference's own GPU code on the same instance and GPU: a baseline leg, like
+    cpu_baseline (oracle/_ref holds test infrastructure and is never on the engine's
+    path).
+      cuda_prototype: the reference's CUDA prototype (cuda/src/sankhya_cuda_lp.cu:101-437,
+        thread-per-row SpMV and an atomicAdd transpose, recompiled for sm_100a) through
+        the same entry point with the same steps, host arrays; the marginal wall time of
+        one iteration and its algorithmic GB/s, beside the engine's measured the same way;
+      gpupdlp: the reference C++ core's GPU PDLP (src/cuda/GpuPdlp.cpp over cuSPARSE
+        CSR SpMV, with its first-order driver's Ruiz + Pock-Chambolle scaling) to 1e-6
+        relative KKT, beside the engine's FP64 PDLP to the same tolerance."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    m, n, nnz = inst["m"], inst["n"], int(inst["ptr"][-1])
+    byt = iteration_bytes(m, n, nnz)
+    out = {}
+    settings = lambda its: dict(max_iterations=its, check_every=its, tau=0.0, sigma=0.0, theta=1.0, tolerance=1e-12,
+                                time_limit=0.0)
+    host = {k: np.ascontiguousarray(inst[k]) for k in ("c", "rl", "ru", "cl", "cu")}
+
+    def engine_call(its):
+        rc, _, _, _ = E.pdhg(A, host, E.settings(**settings(its)), primal_steps=ps, dual_steps=ds,
+                             entry="preconditioned")
+        if rc != 0:
+            raise RuntimeError(E.last_error())
+
+    eng_ms = _marginal_ms(engine_call)
+    try:
+        R = O.RefCudaPrototype(inst)
+        try:
+            def ref_call(its):
+                rc, _, _ = R.pdhg(settings(its), ps, ds)
+                if rc != 0:
+                    raise RuntimeError(f"reference prototype returned {rc}")
+            ref_ms = _marginal_ms(ref_call)
+        finally:
+            R.close()
+        out["cuda_prototype"] = {"ms_per_iteration": round(ref_ms, 4), "gbs": round(byt / ref_ms / 1e6, 1),
+                                 "engine_ms_per_iteration": round(eng_ms, 4),
+                                 "engine_gbs": round(byt / eng_ms / 1e6, 1),
+                                 "engine_speedup": round(ref_ms / eng_ms, 2),
+                                 "method": "marginal wall time per iteration, 200- vs 100-iteration calls"}
+    except (OSError, FileNotFoundError, RuntimeError) as exc:
+        out["cuda_prototype"] = {"unavailable": str(exc)}
+    try:
         t0 = time.perf_counter()
-        rc, x, y, r = E.pdlp_solve(A, inst, s)
+        x, st = O.ref_gpupdlp(inst, eps=1e-6, max_iterations=20_000_000, time_limit=limit_s, scale=True)
         wall = time.perf_counter() - t0
-        out[name] = {"seconds": round(wall, 3), "status": r["status"], "iterations": r["iterations"],
-                     "refinements": r["refinements"], "objective": _finite(np.dot(inst["c"], x)),
-                     "kkt": [_finite(r[k]) for k in ("relative_primal_residual", "relative_dual_residual",
-                                                     "relative_gap")]}
-    ref_obj = out["fp64"]["objective"]
-    for name in ("fp32_refined", "halpern_fp64", "halpern_fp32_refined"):
-        if out["fp64"]["status"] == 0 and out[name]["status"] == 0 and out[name]["seconds"] > 0:
-            out[f"speedup_{name}_vs_fp64"] = round(out["fp64"]["seconds"] / out[name]["seconds"], 3)
-        # the accuracy side of the target: objective against the FP64 run's, relative
-        obj = out[name]["objective"]
-        out[name]["objective_rel_diff_vs_fp64"] = (
-            None if obj is None or ref_obj is None else _finite(abs(obj - ref_obj) / (1.0 + abs(ref_obj))))
+        out["gpupdlp"] = {"seconds": round(wall, 3), "converged": st["converged"], "iterations": st["iterations"],
+                          "solver_seconds": round(st["seconds"], 3), "objective": _finite(np.dot(inst["c"], x)),
+                          "kkt": [_finite(st[k]) for k in ("relative_primal_residual", "relative_dual_residual",
+                                                           "relative_gap")], "eps": 1e-6, "time_limit_s": limit_s}
+    except (OSError, FileNotFoundError, RuntimeError) as exc:
+        out["gpupdlp"] = {"unavailable": str(exc)}
+    return out
+
+
+ORACLE_OBJECTIVE = os.path.join(ROOT, "tests", "golden", "objective_lp_config1.json")
+
+
+def oracle_objective():
+    """The FP64 objective of the bench instance solved to 1e-9 relative KKT (tests/golden,
+    written by tests/golden/make_config1_objective.py), or None where it is absent."""
+    try:
+        with open(ORACLE_OBJECTIVE) as f:
+            return float(json.load(f)["objective"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def _pdlp_run(E, A, inst, eps, precision, algorithm, limit_s, oracle):
+    s = E.pdlp_default_settings()
+    s.eps_optimal, s.precision, s.time_limit, s.max_iterations = eps, precision, limit_s, 20_000_000
+    s.algorithm = algorithm
+    t0 = time.perf_counter()
+    rc, x, y, r = E.pdlp_solve(A, inst, s)
+    wall = time.perf_counter() - t0
+    obj = _finite(np.dot(inst["c"], x))
+    out = {"seconds": round(wall, 3), "status": r["status"], "iterations": r["iterations"],
+           "restarts": r["restarts"], "refinements": r["refinements"], "objective": obj,
+           "kkt": [_finite(r[k]) for k in ("relative_primal_residual", "relative_dual_residual", "relative_gap")]}
+    if oracle is not None and obj is not None:
+        out["objective_rel_err_vs_oracle"] = _finite(abs(obj - oracle) / (1.0 + abs(oracle)))
+    return out
+
+
+def time_to_kkt(E, A, inst, eps_list=(1e-4, 1e-6, 1e-8), limit_s=120.0, halpern=False):
+    """Wall time of sankhya_b200_pdlp_solve to each relative-KKT tolerance on the same
+    instance: plain FP64 PDLP (GpuPdlp's restarted adaptive loop) versus FP32 inner
+    iterations refined in FP64 at every restart. Host arrays in and out, scaling
+    included. Each run's objective is compared with the FP64 oracle value of the
+    instance (solved to 1e-9 by two independent FP64 solvers) where it is present.
+    With halpern, the reflected restarted Halpern loop runs at the middle tolerance."""
+    oracle = oracle_objective()
+    out = {"relative_kkt": "max(primal, dual, gap) as in GpuPdlp", "oracle_objective": oracle,
+           "oracle": "tests/golden/objective_lp_config1.json (FP64 PDLP to 1e-9: engine, and the reference's GpuPdlp)"}
+    for eps in eps_list:
+        key = f"eps_{eps:.0e}"
+        row = {"fp64": _pdlp_run(E, A, inst, eps, E.FP64, E.PDLP_ADAPTIVE, limit_s, oracle),
+               "fp32_refined": _pdlp_run(E, A, inst, eps, E.FP32_REFINE, E.PDLP_ADAPTIVE, limit_s, oracle)}
+        if halpern and eps == eps_list[len(eps_list) // 2]:
+            row["halpern_fp64"] = _pdlp_run(E, A, inst, eps, E.FP64, E.PDLP_HALPERN, limit_s, oracle)
+        for name in [k for k in row if k != "fp64"]:
+            if row["fp64"]["status"] == 0 and row[name]["status"] == 0 and row[name]["seconds"] > 0:
+                row[f"speedup_{name}_vs_fp64"] = round(row["fp64"]["seconds"] / row[name]["seconds"], 3)
+        out[key] = row
     return out
 
 
@@ -250,7 +359,7 @@ def run_reference(args, world, rank):
     I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
     inst = I.lp_config1(SEED)
     nnz = int(inst["ptr"][-1])
-    per_step = 2  # iterations of the reference loop per step: bounded sample of the workload
+    per_step = REFERENCE_ITERS_PER_CALL  # the same calls as the engine line's cpu_baseline sample
     core = reference_core()
     for _ in range(args.warmup):
         reference_loop_gbs(inst, 1, core)
@@ -363,6 +472,13 @@ def run_engine(args, world, rank, local):
                                                                                   "matrix_create": round(create_s, 3)}}
     if world == 1 and not args.no_time_to_kkt:
         line["time_to_kkt"] = time_to_kkt(E, A, inst)
+    if world == 1 and not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_baseline(E, A, inst, ps, ds)
+        ttk = line.get("time_to_kkt", {}).get("eps_1e-06", {}).get("fp64", {})
+        g = line["reference_gpu"].get("gpupdlp", {})
+        if ttk.get("status") == 0 and g.get("converged") == 1:
+            g["engine_fp64_seconds"] = ttk["seconds"]
+            g["engine_speedup"] = round(g["seconds"] / ttk["seconds"], 2)
     if world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(inst)
@@ -531,6 +647,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-time-to-kkt", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference GPU baseline legs")
     ap.add_argument("--batches", action="store_true", help="batched workloads instead of the headline line")
     ap.add_argument("--small", action="store_true", help="with --batches: 64 nodes and 256 LPs")
     ap.add_argument("--nodes-only", action="store_true", help="with --batches: the shared-matrix node batch only")

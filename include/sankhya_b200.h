@@ -135,7 +135,15 @@ enum {
 
 enum {
     SANKHYA_B200_FP64 = 0,       /* FP64 everywhere                                  */
-    SANKHYA_B200_FP32_REFINE = 1 /* FP32 inner iterations, FP64 refinement residuals */
+    SANKHYA_B200_FP32_REFINE = 1 /* FP32 inner iterations, FP64 refinement residuals:
+                                    with the adaptive step, the iterations run in FP32 on
+                                    deviations from an FP64 center that moves to the
+                                    restart point at every restart (one refinement: the
+                                    problem's residual data b - A x_c and c + A'y_c are
+                                    re-formed in FP64 there); restart and KKT decisions
+                                    use FP64 residuals of center + deviation. With the
+                                    Halpern loop or the fixed step: an FP32 phase to
+                                    1e-4, then an FP64 finish.                         */
 };
 
 enum {
@@ -180,7 +188,9 @@ typedef struct SankhyaB200PdlpResult {
     int restarts;
     int rejected_steps;
     int host_syncs;
-    int refinements;       /* outer refinement passes (FP32_REFINE)               */
+    int refinements;       /* FP32_REFINE: FP64 centers formed (the start and one per
+                              restart) with the adaptive step; 1 when the FP64 finish
+                              ran after an FP32 phase otherwise; 0 for FP64            */
     double primal_objective;
     double dual_objective;
     double relative_primal_residual;

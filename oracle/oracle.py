@@ -297,6 +297,52 @@ def ref_gpupdlp(inst, eps=1e-8, max_iterations=500000, restart_period=64, power_
     return x, {k: getattr(st, k) for k, _ in RefPdlpStats._fields_}
 
 
+class RefCudaCsr(C.Structure):
+    """Layout of the reference's SankhyaCudaCSR (cuda/include/sankhya_cuda.h)."""
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("nnz", C.c_int), ("device_row_offsets", C.c_void_p),
+                ("device_column_indices", C.c_void_p), ("device_values", C.c_void_p)]
+
+
+class RefCudaPrototype:
+    """The reference's CUDA prototype (cuda/src/sankhya_cuda*.cu built for sm_100a into
+    _ref/libsankhya_cuda_ref.so) holding one matrix on the current device; `pdhg` is its
+    sankhya_cuda_qp_pdhg_preconditioned (LP: no Hessian, no diagonal). Needs a GPU."""
+
+    def __init__(self, inst):
+        L = load("ref_cuda")
+        P = C.POINTER
+        L.sankhya_cuda_csr_create.argtypes = [P(RefCudaCsr), C.c_int, C.c_int, C.c_int, iptr, iptr, dptr]
+        L.sankhya_cuda_csr_destroy.argtypes = [P(RefCudaCsr)]
+        L.sankhya_cuda_csr_destroy.restype = None
+        L.sankhya_cuda_qp_pdhg_preconditioned.argtypes = [P(RefCudaCsr), P(RefCudaCsr), dptr, dptr, dptr, dptr,
+                                                          dptr, dptr, dptr, dptr, LPSettings, dptr, P(LPResult)]
+        L.sankhya_cuda_last_error.restype = C.c_char_p
+        self.L = L
+        self.keep = _Keep()
+        self.h = RefCudaCsr()
+        k = self.keep
+        rc = L.sankhya_cuda_csr_create(C.byref(self.h), inst["m"], inst["n"], int(inst["ptr"][-1]),
+                                       _p(k.i(inst["ptr"]), iptr), _p(k.i(inst["idx"]), iptr), _p(k.d(inst["val"])))
+        if rc != 0:
+            raise RuntimeError("reference sankhya_cuda_csr_create failed: " + L.sankhya_cuda_last_error().decode())
+        self.arrays = {name: k.d(inst[name]) for name in ("c", "rl", "ru", "cl", "cu")}
+        self.n = inst["n"]
+
+    def pdhg(self, settings: dict, primal_steps, dual_steps):
+        a, k = self.arrays, self.keep
+        x = np.zeros(self.n)
+        res = LPResult()
+        rc = self.L.sankhya_cuda_qp_pdhg_preconditioned(
+            C.byref(self.h), None, None, _p(a["c"]), _p(a["rl"]), _p(a["ru"]), _p(a["cl"]), _p(a["cu"]),
+            _p(k.d(primal_steps)), _p(k.d(dual_steps)), LPSettings(**settings), _p(x), C.byref(res))
+        return rc, x, res.as_dict()
+
+    def close(self):
+        if self.h is not None:
+            self.L.sankhya_cuda_csr_destroy(C.byref(self.h))
+            self.h = None
+
+
 def pow2_scale(inst, passes=4):
     lib = load("oracle")
     keep = _Keep()

@@ -37,7 +37,7 @@ class _FakeEngine:
         import time
         time.sleep(0.002)   # wall times are rounded to milliseconds
         status, x = self.answers[(s.precision, s.algorithm)]
-        r = {"status": status, "iterations": 640, "refinements": int(s.precision == 1),
+        r = {"status": status, "iterations": 640, "restarts": 3, "refinements": 4 * int(s.precision == 1),
              "relative_primal_residual": 1e-7, "relative_dual_residual": 1e-7, "relative_gap": 1e-7}
         return 0, np.asarray(x, dtype=float), None, r
 
@@ -50,33 +50,65 @@ def test_iteration_bytes_are_the_two_launches():
     assert b.primal_bytes(m, n, nnz) == 12 * nnz + 4 * (n + 1) + 8 * m + 48 * n
 
 
-def test_time_to_kkt_reports_speedups_and_objective_agreement():
+def test_time_to_kkt_reports_speedups_and_objective_error(monkeypatch):
+    """One row per tolerance: FP64 and FP32-refined runs, the speed-up where both
+    converged, and each objective's relative error against the oracle value."""
     b = _bench()
+    monkeypatch.setattr(b, "oracle_objective", lambda: -1.0)
     inst = {"c": np.array([1.0, -2.0])}
     E = _FakeEngine({(0, 0): (0, [1.0, 1.0]), (1, 0): (0, [1.0, 1.0 + 1e-7]),
                      (0, 1): (1, [0.0, 0.0]), (1, 1): (0, [np.nan, 0.0])})
-    out = b.time_to_kkt(E, None, inst)
-    assert out["fp64"]["objective"] == -1.0
-    assert abs(out["fp32_refined"]["objective_rel_diff_vs_fp64"] - 2e-7 / 2.0) < 1e-15
-    assert "speedup_fp32_refined_vs_fp64" in out
-    assert "speedup_halpern_fp64_vs_fp64" not in out          # that run did not converge
-    assert out["halpern_fp64"]["objective_rel_diff_vs_fp64"] == 0.5
-    assert out["halpern_fp32_refined"]["objective_rel_diff_vs_fp64"] is None   # NaN is not JSON
+    out = b.time_to_kkt(E, None, inst, eps_list=(1e-4, 1e-6, 1e-8), halpern=True)
+    assert out["oracle_objective"] == -1.0
+    for key in ("eps_1e-04", "eps_1e-06", "eps_1e-08"):
+        row = out[key]
+        assert row["fp64"]["objective"] == -1.0 and row["fp64"]["objective_rel_err_vs_oracle"] == 0.0
+        assert abs(row["fp32_refined"]["objective_rel_err_vs_oracle"] - 2e-7 / 2.0) < 1e-15
+        assert row["fp32_refined"]["refinements"] == 4
+        assert "speedup_fp32_refined_vs_fp64" in row
+    assert "halpern_fp64" in out["eps_1e-06"] and "halpern_fp64" not in out["eps_1e-04"]
+    assert "speedup_halpern_fp64_vs_fp64" not in out["eps_1e-06"]     # that run did not converge
+    assert out["eps_1e-06"]["halpern_fp64"]["objective_rel_err_vs_oracle"] == 0.5
     json.dumps(out, allow_nan=False)
 
 
-def test_time_to_kkt_survives_instant_solves():
+def test_time_to_kkt_without_oracle_and_nan_objective(monkeypatch):
+    """No oracle file: no error entries; a NaN objective is reported as null (strict JSON)."""
+    b = _bench()
+    monkeypatch.setattr(b, "oracle_objective", lambda: None)
+    E = _FakeEngine({(0, 0): (0, [1.0]), (1, 0): (0, [np.nan])})
+    out = b.time_to_kkt(E, None, {"c": np.array([1.0])}, eps_list=(1e-6,))
+    row = out["eps_1e-06"]
+    assert "objective_rel_err_vs_oracle" not in row["fp64"]
+    assert row["fp32_refined"]["objective"] is None
+    json.dumps(out, allow_nan=False)
+
+
+def test_time_to_kkt_survives_instant_solves(monkeypatch):
     """A solve faster than the millisecond rounding gives no speed-up entry, not a
     division by zero."""
     b = _bench()
+    monkeypatch.setattr(b, "oracle_objective", lambda: 1.0)
     E = _FakeEngine({(p, a): (0, [1.0]) for p in (0, 1) for a in (0, 1)})
     E.pdlp_solve = lambda A, inst, s: (0, np.array([1.0]), None,
-                                       {"status": 0, "iterations": 64, "refinements": 0,
+                                       {"status": 0, "iterations": 64, "restarts": 0, "refinements": 0,
                                         "relative_primal_residual": 0.0, "relative_dual_residual": 0.0,
                                         "relative_gap": 0.0})
-    out = b.time_to_kkt(E, None, {"c": np.array([1.0])})
-    assert all(out[k]["objective_rel_diff_vs_fp64"] == 0.0 for k in ("fp32_refined", "halpern_fp64"))
+    out = b.time_to_kkt(E, None, {"c": np.array([1.0])}, eps_list=(1e-6,))
+    row = out["eps_1e-06"]
+    assert "speedup_fp32_refined_vs_fp64" not in row
+    assert row["fp32_refined"]["objective_rel_err_vs_oracle"] == 0.0
     json.dumps(out, allow_nan=False)
+
+
+def test_oracle_objective_file_parses():
+    """The committed oracle value (where present) is a finite float the bench can use."""
+    b = _bench()
+    v = b.oracle_objective()
+    if os.path.exists(b.ORACLE_OBJECTIVE):
+        assert v is not None and np.isfinite(v)
+    else:
+        assert v is None
 
 
 def test_clock_summary_parses_nvidia_smi_rows():

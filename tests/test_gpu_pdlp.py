@@ -126,12 +126,32 @@ def test_fp32_refined_reaches_simplex_objective(engine, instances, golden_dir, n
 def test_fp32_refined_agrees_with_fp64_on_power_law(engine, instances):
     inst = instances.lp_powerlaw(21, 4000, 8000, 80000)
     A = engine.Matrix.from_instance(inst)
-    rc64, x64, y64, r64 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-5, time_limit=60.0))
-    rc32, x32, y32, r32 = engine.pdlp_solve(A, inst, settings(engine, precision=engine.FP32_REFINE, eps_optimal=1e-5,
+    rc64, x64, y64, r64 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-6, time_limit=60.0))
+    rc32, x32, y32, r32 = engine.pdlp_solve(A, inst, settings(engine, precision=engine.FP32_REFINE, eps_optimal=1e-6,
                                                               time_limit=60.0))
     assert rc64 == 0 and rc32 == 0 and r64["status"] == 0 and r32["status"] == 0, (r64, r32)
     o64, o32 = float(np.dot(inst["c"], x64)), float(np.dot(inst["c"], x32))
-    assert abs(o64 - o32) <= 1e-4 * (1 + abs(o64))
+    assert abs(o64 - o32) <= 1e-6 * (1 + abs(o64))
+
+
+@pytest.mark.parametrize("eps", [1e-6, 1e-8])
+def test_fp32_centered_loop_follows_fp64(engine, instances, eps):
+    """FP32 iterations on deviations from an FP64 center that moves to each restart
+    point: the restart decisions see FP64 residuals of the combined point, so the
+    solve takes about the FP64 solve's iterations (plain FP32 arithmetic takes several
+    times more on such instances) and reaches FP64 accuracy; every restart is one
+    refinement."""
+    inst = instances.lp_uniform(3, 5000, 10000, 5)
+    A = engine.Matrix.from_instance(inst)
+    rc64, x64, _, r64 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=eps, time_limit=60.0))
+    rc32, x32, _, r32 = engine.pdlp_solve(A, inst, settings(engine, precision=engine.FP32_REFINE, eps_optimal=eps,
+                                                            time_limit=60.0))
+    assert rc64 == rc32 == 0 and r64["status"] == r32["status"] == 0, (r64, r32)
+    assert r32["refinements"] == r32["restarts"] + 1 and r32["refinements"] > 1
+    assert r32["iterations"] <= 1.15 * r64["iterations"] + 256, (r32["iterations"], r64["iterations"])
+    assert max(r32["relative_primal_residual"], r32["relative_dual_residual"], r32["relative_gap"]) <= eps
+    o64, o32 = float(np.dot(inst["c"], x64)), float(np.dot(inst["c"], x32))
+    assert abs(o64 - o32) <= 10 * eps * (1 + abs(o64)), (o64, o32)
 
 
 # ------------------------------------------------------- reflected Halpern PDHG option

@@ -1,5 +1,5 @@
 // Restarted adaptive PDLP behind sankhya_b200_pdlp_solve, in FP64 or with
-// FP32 inner iterations inside an FP64 iterative-refinement loop.
+// FP32 inner iterations inside an FP64 iterative-refinement loop (FP32_REFINE).
 //
 // The algorithm is the reference's GpuPdlp (src/cuda/GpuPdlp.cpp:179-534,
 // src/cuda/PdlpKernels.cu:71-518): power-iteration ||A||_2, eta = 0.9/||A||,
@@ -21,14 +21,25 @@
 // average iterate (PdlpKernels.cu:101-209, fused into the two products), and
 // one small copy to the host, which makes the restart decision.
 //
-// FP32_REFINE: the iterations run with FP32 matrix values and vectors (FP32
-// accumulation in the products, FP64 for the restart / KKT reductions) on the
-// scaled problem until the FP64-evaluated relative KKT reaches max(eps, 1e-4);
-// the point, the primal weight and the step size then seed an FP64 finish to
-// eps. (A correction-LP refinement in the manner of Gleixner, Steffy and Wolter
-// was tried first and stalled on boxed LPs: the refined problem's bound terms
-// ap (u - x) multiply the FP32 reduced-cost noise in the dual objective, so its
-// relative gap never reached the inner tolerance.)
+// FP32_REFINE (adaptive step): iterative refinement at every restart. The FP32
+// iterations (FP32 matrix values and vectors, FP32 accumulation in the products)
+// run on deviations (dx, dy) from an FP64 center (x_c, y_c). At the start and at
+// each restart the center moves to the restart point and the FP32 problem is
+// re-formed around it in FP64 (the refinement residuals): cost c + A'y_c, column
+// bounds minus x_c, row bounds minus A x_c, each rounded once to FP32. Shifting the
+// primal box is exact; the dual prox is taken of the absolute dual y_c + v in FP64
+// (the row bounds' support function does not move with the shift), so the FP32
+// loop solves the same saddle problem as the FP64 one. The window-end residuals
+// and the KKT / restart decisions are FP64 sums over center + deviation of the
+// scaled FP64 problem. Because the deviations shrink as the solve converges, FP32
+// rounding stays relative to the step, not to the iterate, and the loop takes the
+// FP64 loop's iterations and reaches its accuracy (plain FP32 iterates stall the
+// adaptive step: its interaction term dy'A dx is a difference of O(1) FP32
+// products). The Halpern loop and the fixed step keep an FP32 phase to 1e-4
+// followed by an FP64 finish.
+// (A Gleixner-Steffy-Wolter correction LP with scaled residuals was tried first:
+// it re-solves the slow tail of PDLP at every pass and made no progress on boxed
+// LPs; re-centering without scaling keeps the restart schedule running instead.)
 #include "engine.cuh"
 
 #include <cstddef>
@@ -72,13 +83,16 @@ __device__ __forceinline__ T clampf(T v, T lo, T hi) {
 
 // ------------------------------------------------------------ iteration kernels
 
-// K1 (PdlpKernels.cu:499-518 commit, then :377-389 dual candidate)
+// K1 (PdlpKernels.cu:499-518 commit, then :377-389 dual candidate). With
+// y_center (the centered FP32 loop) y, ax, ax_prev are deviations from an FP64
+// center and rl / ru the row bounds shifted by A x_center: the prox is taken of
+// the absolute dual y_center + v, in FP64, and the candidate stored as a deviation.
 template <class T>
 __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, T* __restrict__ x,
                               const T* __restrict__ x_cand, T* __restrict__ x_sum, T* __restrict__ y,
                               T* __restrict__ y_cand, T* __restrict__ y_sum, T* __restrict__ ax, T* __restrict__ ax_prev,
                               const T* __restrict__ ax_cand, const T* __restrict__ rl, const T* __restrict__ ru,
-                              int make_candidate) {
+                              const double* __restrict__ y_center, int make_candidate) {
     const bool acc = st->accepted != 0.0;
     const T sigma = static_cast<T>(st->eta * st->omega);
     const int stride = blockDim.x * gridDim.x;
@@ -96,7 +110,14 @@ __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, T* __res
         }
         if (make_candidate) {
             const T v = yi + sigma * (T(2) * axi - axp);
-            y_cand[i] = v - sigma * clampf<T>(v / sigma, rl[i], ru[i]);
+            if (y_center) {
+                const double s = static_cast<double>(sigma), vd = static_cast<double>(v);
+                const double w = (y_center[i] + vd) / s;
+                y_cand[i] = static_cast<T>(vd - s * clampf<double>(w, static_cast<double>(rl[i]),
+                                                                    static_cast<double>(ru[i])));
+            } else {
+                y_cand[i] = v - sigma * clampf<T>(v / sigma, rl[i], ru[i]);
+            }
         }
     }
     if (acc) {
@@ -456,6 +477,119 @@ struct ResColsEpi {
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
 };
+
+// The same sums for the centered FP32 loop, evaluated in FP64 on the combined point
+// (FP64 center + FP32 deviation) against the scaled FP64 problem: A x = ax_center +
+// (A dx), A'y = rc_center - c + (A'dy) (rc_center = c + A'y_center), x = x_center + dx,
+// y = y_center + dy. The restart reference is the center itself, so the moves since
+// the last restart are the deviations.
+template <class T>
+struct ResRowsCenteredEpi {
+    const T* __restrict__ dy;
+    const double* __restrict__ y_center;
+    const double* __restrict__ ax_center;
+    const double* __restrict__ rl;
+    const double* __restrict__ ru;
+    T* __restrict__ ax_out;  // may be null: receives A dx
+    double* __restrict__ partial;
+    using Acc = Slots<5, 0xFu>;
+    __device__ __forceinline__ void row(int i, T adx, Acc& acc) const {
+        if (ax_out) ax_out[i] = adx;
+        const double d = static_cast<double>(dy[i]);
+        const double axi = ax_center[i] + static_cast<double>(adx), lo = rl[i], hi = ru[i], yi = y_center[i] + d;
+        const double pr = axi - fmin(fmax(axi, lo), hi);
+        acc.add(0, pr * pr);
+        acc.add(1, yi * yi);
+        acc.add(2, d * d);
+        double support = 0.0;
+        if (yi > 0.0) support = isfinite(hi) ? yi * hi : 0.0;
+        else if (yi < 0.0) support = isfinite(lo) ? yi * lo : 0.0;
+        acc.add(3, -support);
+        acc.max(4, fabs(pr));
+    }
+    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
+};
+
+template <class T>
+struct ResColsCenteredEpi {
+    const T* __restrict__ dx;
+    const double* __restrict__ x_center;
+    const double* __restrict__ rc_center;
+    const double* __restrict__ c;
+    const double* __restrict__ cl;
+    const double* __restrict__ cu;
+    double* __restrict__ partial;
+    using Acc = Slots<6, 0x1Fu>;
+    __device__ __forceinline__ void row(int j, T atdy, Acc& acc) const {
+        const double d = static_cast<double>(dx[j]);
+        const double xj = x_center[j] + d, lo = cl[j], hi = cu[j], cj = c[j];
+        const double r = rc_center[j] + static_cast<double>(atdy);
+        acc.add(2, cj * xj);
+        acc.add(3, xj * xj);
+        acc.add(4, d * d);
+        const bool lf = isfinite(lo), hf = isfinite(hi);
+        double viol = 0.0, term = 0.0;
+        if (lf && hf) {
+            term = fmin(r * lo, r * hi);
+        } else if (lf) {
+            viol = fmax(0.0, -r);
+            term = fmax(0.0, r) * lo;
+        } else if (hf) {
+            viol = fmax(0.0, r);
+            term = fmin(0.0, r) * hi;
+        } else {
+            viol = fabs(r);
+        }
+        acc.add(0, viol * viol);
+        acc.add(1, term);
+        acc.max(5, fabs(xj - fmin(fmax(xj - r, lo), hi)));
+    }
+    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
+};
+
+// Re-centering of the FP32 loop: the center moves by the deviation `from` (the
+// restart point), x kept inside its bounds.
+template <class T>
+__global__ void k_recenter(int n, int m, const T* __restrict__ from_x, const T* __restrict__ from_y,
+                           double* __restrict__ xc, double* __restrict__ yc, const double* __restrict__ cl,
+                           const double* __restrict__ cu) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
+        xc[j] = fmin(fmax(xc[j] + static_cast<double>(from_x[j]), cl[j]), cu[j]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) yc[i] += static_cast<double>(from_y[i]);
+}
+
+// FP32 data of the problem around the center (FP64 in, one rounding out):
+// c + A'yc, column bounds minus xc, row bounds minus A xc; infinite bounds stay infinite.
+__global__ void k_frame(int n, int m, const double* __restrict__ c, const double* __restrict__ aty_c,
+                        const double* __restrict__ cl, const double* __restrict__ cu, const double* __restrict__ xc,
+                        const double* __restrict__ rl, const double* __restrict__ ru, const double* __restrict__ ax_c,
+                        double* __restrict__ rc_c, float* __restrict__ c32, float* __restrict__ cl32,
+                        float* __restrict__ cu32, float* __restrict__ rl32, float* __restrict__ ru32) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const double r = c[j] + aty_c[j];
+        rc_c[j] = r;
+        c32[j] = static_cast<float>(r);
+        cl32[j] = static_cast<float>(cl[j] - xc[j]);
+        cu32[j] = static_cast<float>(cu[j] - xc[j]);
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        rl32[i] = static_cast<float>(rl[i] - ax_c[i]);
+        ru32[i] = static_cast<float>(ru[i] - ax_c[i]);
+    }
+}
+
+// Deviations, running sums and products back to zero after a re-centering; the
+// accepted-step count at the restart is recorded as k_restart does.
+template <class T>
+__global__ void k_zero_deviation(int n, int m, T* __restrict__ x, T* __restrict__ x_sum, T* __restrict__ y,
+                                 T* __restrict__ y_sum, T* __restrict__ ax, T* __restrict__ ax_prev, PdlpState* st) {
+    const int stride = blockDim.x * gridDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) x[j] = x_sum[j] = T(0);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y[i] = y_sum[i] = ax[i] = ax_prev[i] = T(0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->accepted_at_restart = st->accept_count;
+}
 
 // out[0..7] in the reference's PdlpResiduals order (PdlpKernels.cuh), then the
 // step state, then out[12] max primal residual, out[13] max column KKT residual;
@@ -921,6 +1055,17 @@ struct LoopParams {
     void* cancel_context = nullptr;
 };
 
+// The FP64 side of the centered FP32 loop: the scaled FP64 problem, the center
+// (x_center, y_center: the last restart point, which is also the refinement
+// point), its products and the FP32 frame data the iterations run on.
+struct Centered {
+    TileCsr A, AT;  // scaled FP64 matrix
+    const double *c = nullptr, *cl = nullptr, *cu = nullptr, *rl = nullptr, *ru = nullptr;
+    double *xc = nullptr, *yc = nullptr, *ax_c = nullptr, *aty_c = nullptr, *rc_c = nullptr;
+    float *c32 = nullptr, *cl32 = nullptr, *cu32 = nullptr, *rl32 = nullptr, *ru32 = nullptr;
+    int grid_a = 1, grid_at = 1;
+};
+
 struct LoopStats {
     long long iterations = 0;
     int restarts = 0, syncs = 0;
@@ -945,8 +1090,15 @@ struct Core {
     double* host = nullptr;
     int grid_k2 = 1, grid_k3 = 1, grid_rr = 1, grid_rc = 1, grid_df = 1, grid_pf = 1;
     int grid_ph = 1, grid_dh = 1, grid_pt = 1, grid_dt = 1;
+    int grid_rrc = 1, grid_rcc = 1;
     int launches = 0;
     std::vector<cudaGraphExec_t> graphs;
+    // Centered mode (FP32 iterations of the FP32_REFINE precision): x, y, ax and the
+    // sums are deviations from ctr's FP64 center; the center moves to the restart
+    // point at every restart (one refinement), and the window-end residuals are
+    // taken in FP64 on center + deviation.
+    const Centered* ctr = nullptr;
+    int recenters = 0;
     Core() = default;
     Core(const Core&) = delete;
     Core& operator=(const Core&) = delete;
@@ -996,6 +1148,8 @@ struct Core {
         grid_dh = tiled_grid<DualHalpernEpi<T>, T>(A);
         grid_pt = tiled_grid<PrimalTEpi<T>, T>(AT);
         grid_dt = tiled_grid<DualTEpi<T>, T>(A);
+        grid_rrc = tiled_grid<ResRowsCenteredEpi<T>, T>(A);
+        grid_rcc = tiled_grid<ResColsCenteredEpi<T>, T>(AT);
         for (auto g : graphs)
             if (g) cudaGraphExecDestroy(g);
         graphs.clear();
@@ -1003,6 +1157,16 @@ struct Core {
 
     // Residual sums of (xv, yv) into out[0..13]; ax_out / aty_out optional.
     void residuals(const T* xv, const T* yv, T* ax_out, T* aty_out, double* out, int clear_accept) {
+        if (ctr) {
+            const int nbr = A.ntiles ? grid_rrc : 0, nbc = AT.ntiles ? grid_rcc : 0;
+            launch_tiled(A, xv, ResRowsCenteredEpi<T>{yv, ctr->yc, ctr->ax_c, ctr->rl, ctr->ru, ax_out, part_a},
+                         stream, grid_rrc);
+            launch_tiled(AT, yv, ResColsCenteredEpi<T>{xv, ctr->xc, ctr->rc_c, ctr->c, ctr->cl, ctr->cu, part_b},
+                         stream, grid_rcc);
+            k_res_combine<<<1, kThreads, 0, stream>>>(part_a, nbr, part_b, nbc, out, st, clear_accept);
+            launches += 3;
+            return;
+        }
         const int nbr = A.ntiles ? grid_rr : 0, nbc = AT.ntiles ? grid_rc : 0;
         launch_tiled(A, xv, ResRowsEpi<T>{yv, y_restart, rl, ru, ax_out, part_a}, stream, grid_rr);
         launch_tiled(AT, yv, ResColsEpi<T>{xv, x_restart, c, cl, cu, aty_out, part_b}, stream, grid_rc);
@@ -1013,7 +1177,7 @@ struct Core {
     void adaptive_iteration(bool make_candidate) {
         k_commit_dual<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, x, x_cand, x_sum, y, y_cand, y_sum,
                                                                       ax, ax_prev, ax_cand, rl, ru,
-                                                                      make_candidate ? 1 : 0);
+                                                                      ctr ? ctr->yc : nullptr, make_candidate ? 1 : 0);
         ++launches;
         if (!make_candidate) return;
         launch_tiled(AT, y_cand, PrimalCandEpi<T>{st, x, c, cl, cu, x_cand, part_c}, stream, grid_k2);
@@ -1061,6 +1225,29 @@ struct Core {
         B200_TRY(cudaGraphLaunch(exec, stream), "graph launch");
         launches += (adaptive ? 3 * period + 1 : 2 * period) + 7;
         return 0;
+    }
+
+    // Centered mode: products of the FP64 center and the FP32 frame data around it.
+    void build_frame() {
+        launch_tiled(ctr->A, ctr->xc, StoreEpi{ctr->ax_c}, stream, ctr->grid_a);
+        launch_tiled(ctr->AT, ctr->yc, StoreEpi{ctr->aty_c}, stream, ctr->grid_at);
+        k_frame<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, ctr->c, ctr->aty_c, ctr->cl, ctr->cu, ctr->xc,
+                                                             ctr->rl, ctr->ru, ctr->ax_c, ctr->rc_c, ctr->c32,
+                                                             ctr->cl32, ctr->cu32, ctr->rl32, ctr->ru32);
+        launches += 3;
+        ++recenters;
+    }
+
+    // Centered mode: the center moves by the deviation (fx, fy); with rebuild the
+    // frame follows and the deviations restart at zero (a restart), else the
+    // center alone is updated (the final point).
+    void recenter(const T* fx, const T* fy, bool rebuild) {
+        k_recenter<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, fx, fy, ctr->xc, ctr->yc, ctr->cl, ctr->cu);
+        ++launches;
+        if (!rebuild) return;
+        build_frame();
+        k_zero_deviation<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, x, x_sum, y, y_sum, ax, ax_prev, st);
+        ++launches;
     }
 
     // One Halpern window: `period` anchored steps, then T at the window's end
@@ -1189,6 +1376,13 @@ struct Core {
         if (lp.halpern) return run_halpern(lp, out);
         const size_t nb = sizeof(T) * static_cast<size_t>(std::max(n, 1));
         const size_t mb = sizeof(T) * static_cast<size_t>(std::max(m, 1));
+        if (ctr) {
+            // the start point is the center (its products and frame); deviations zero
+            if (!lp.adaptive) return fail_msg("the centered FP32 loop needs the adaptive step");
+            build_frame();
+            B200_TRY(cudaMemsetAsync(x, 0, nb, stream), "zero");
+            B200_TRY(cudaMemsetAsync(y, 0, mb, stream), "zero");
+        }
         for (T* v : {x_sum, x_cand, x_avg, aty}) cudaMemsetAsync(v, 0, nb, stream);
         for (T* v : {y_sum, y_cand, y_avg, ax_cand, ax_avg}) cudaMemsetAsync(v, 0, mb, stream);
         B200_TRY(cudaMemcpyAsync(x_restart, x, nb, cudaMemcpyDeviceToDevice, stream), "copy");
@@ -1252,14 +1446,17 @@ struct Core {
                     B200_TRY(cudaMemcpyAsync(y, y_avg, mb, cudaMemcpyDeviceToDevice, stream), "copy");
                 }
                 out->converged = true;
+                if (ctr) recenter(x, y, false);
                 break;
             }
             if (lp.deadline > 0.0 && now_s() > lp.deadline) {
                 out->timed_out = true;
+                if (ctr) recenter(x, y, false);
                 break;
             }
             if (lp.cancel && lp.cancel(lp.cancel_context) != 0) {
                 out->cancelled = true;
+                if (ctr) recenter(x, y, false);
                 break;
             }
             const double mu = best.worst();
@@ -1269,10 +1466,16 @@ struct Core {
                 static_cast<double>(iterations_since_restart) >= kArtificial * static_cast<double>(iteration);
             mu_previous = mu;
             if (!(sufficient || necessary || artificial)) continue;
-            k_restart<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(
-                n, m, average_better ? 1 : 0, lp.adaptive ? 1 : 0, x, y, x_bar, x_avg, y_avg, ax, ax_prev, ax_avg,
-                x_sum, y_sum, x_restart, y_restart, st);
-            ++launches;
+            if (ctr) {
+                // restart = refinement: the center moves to the restart point, the FP32
+                // problem is re-formed around it in FP64, the deviations restart at zero
+                recenter(average_better ? x_avg : x, average_better ? y_avg : y, true);
+            } else {
+                k_restart<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(
+                    n, m, average_better ? 1 : 0, lp.adaptive ? 1 : 0, x, y, x_bar, x_avg, y_avg, ax, ax_prev,
+                    ax_avg, x_sum, y_sum, x_restart, y_restart, st);
+                ++launches;
+            }
             windows_since_restart = 0;
             iterations_since_restart = 0;
             mu_at_restart = mu;
@@ -1284,6 +1487,8 @@ struct Core {
                 if (std::isfinite(updated)) omega = std::min(kMaxWeight, std::max(kMinWeight, updated));
             }
         }
+        if (ctr && !out->converged && !out->timed_out && !out->cancelled && !out->numeric)
+            recenter(x, y, false);  // iteration limit: the center takes the last point
         out->iterations += iteration;
         out->omega = omega;
         return 0;
@@ -1428,8 +1633,54 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         lp.bound_norm = bound_norm;
         if (hi.run(lp, &stats)) return -1;
         launches += hi.launches;
+    } else if (lp.adaptive && !lp.halpern) {
+        // ------------------------- FP32 iterations around an FP64 center, refined at restarts
+        DevBuf vals32, blob32, cbuf;
+        const size_t nnz = static_cast<size_t>(plan->a.nnz);
+        if (vals32.alloc(nnz * 8 + 1024, "cudaMalloc FP32 values")) return -1;
+        float* a32 = vals32.as<float>();
+        float* at32 = a32 + (nnz + 63) / 64 * 64;
+        k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.A.val, a32);
+        k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.AT.val, at32);
+        const size_t nf = (static_cast<size_t>(n) * 4 + 255) / 256 * 256;
+        const size_t mf = (static_cast<size_t>(m) * 4 + 255) / 256 * 256;
+        const size_t nd = (static_cast<size_t>(n) * 8 + 255) / 256 * 256;
+        const size_t md = (static_cast<size_t>(m) * 8 + 255) / 256 * 256;
+        if (blob32.alloc(3 * nf + 2 * mf + 256, "cudaMalloc FP32 frame")) return -1;
+        if (cbuf.alloc(2 * nd + md + 256, "cudaMalloc FP64 center products")) return -1;
+        char* base = blob32.as<char>();
+        Centered ctr;
+        ctr.A = sc.A;
+        ctr.AT = sc.AT;
+        ctr.c = sc.c; ctr.cl = sc.cl; ctr.cu = sc.cu; ctr.rl = sc.rl; ctr.ru = sc.ru;
+        ctr.xc = hi.x;
+        ctr.yc = hi.y;
+        ctr.aty_c = cbuf.as<double>();
+        ctr.rc_c = reinterpret_cast<double*>(cbuf.as<char>() + nd);
+        ctr.ax_c = reinterpret_cast<double*>(cbuf.as<char>() + 2 * nd);
+        ctr.c32 = reinterpret_cast<float*>(base);
+        ctr.cl32 = reinterpret_cast<float*>(base + nf);
+        ctr.cu32 = reinterpret_cast<float*>(base + 2 * nf);
+        ctr.rl32 = reinterpret_cast<float*>(base + 3 * nf);
+        ctr.ru32 = reinterpret_cast<float*>(base + 3 * nf + mf);
+        ctr.grid_a = tiled_grid<StoreEpi>(sc.A);
+        ctr.grid_at = tiled_grid<StoreEpi>(sc.AT);
+        Core<float> lo;
+        lo.stream = stream;
+        lo.host = hs.p;
+        if (lo.allocate(n, m, sc.sms)) return -1;
+        lo.set_problem(sc.A.with_values<float>(a32), sc.AT.with_values<float>(at32), ctr.c32, ctr.cl32, ctr.cu32,
+                       ctr.rl32, ctr.ru32);
+        lo.ctr = &ctr;
+        lp.eps = s.eps_optimal;
+        lp.max_iterations = s.max_iterations;
+        lp.cost_norm = cost_norm;
+        lp.bound_norm = bound_norm;
+        if (lo.run(lp, &stats)) return -1;
+        refinements = lo.recenters;
+        launches += hi.launches + lo.launches;
     } else {
-        // -------------------------------------- FP32 iterations, then an FP64 finish
+        // ------------- Halpern or fixed-step loop: FP32 iterations, then an FP64 finish
         DevBuf vals32, blob32;
         const size_t nnz = static_cast<size_t>(plan->a.nnz);
         if (vals32.alloc(nnz * 8 + 1024, "cudaMalloc FP32 values")) return -1;
