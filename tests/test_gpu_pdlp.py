@@ -123,6 +123,22 @@ def test_fp32_refined_reaches_simplex_objective(engine, instances, golden_dir, n
     assert abs(obj - ref["objective"]) <= 1e-6 * (1 + abs(ref["objective"])), (obj, ref)
 
 
+@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE"])
+def test_config0_to_1e8_reaches_the_simplex_objective(engine, instances, golden_dir, precision):
+    """The 2,000 x 5,000 LP (instances.lp_config0, seed 0) to 1e-8 relative KKT, FP64
+    and FP32 iterations refined in FP64: the objective matches the reference simplex's
+    (certified by its sk_verify, cross-checked with HiGHS) to 1e-6 relative."""
+    g = json.load(open(os.path.join(golden_dir, "simplex_lp_config0.json")))
+    inst = instances.lp_config0(0)
+    A = engine.Matrix.from_instance(inst)
+    rc, x, y, r = engine.pdlp_solve(A, inst, settings(engine, precision=getattr(engine, precision),
+                                                      eps_optimal=1e-8, time_limit=120.0))
+    assert rc == 0 and r["status"] == 0, r
+    assert max(r["relative_primal_residual"], r["relative_dual_residual"], r["relative_gap"]) <= 1e-8
+    obj = float(np.dot(inst["c"], x))
+    assert abs(obj - g["objective"]) <= 1e-6 * (1 + abs(g["objective"])), (obj, g["objective"])
+
+
 def test_fp32_refined_agrees_with_fp64_on_power_law(engine, instances):
     inst = instances.lp_powerlaw(21, 4000, 8000, 80000)
     A = engine.Matrix.from_instance(inst)

@@ -141,6 +141,30 @@ def test_pdlp_oracle_reaches_simplex_objective(oracle, instances, golden_dir):
     assert abs(obj - ref["objective"]) <= 1e-6 * (1 + abs(ref["objective"]))
 
 
+def test_config0_simplex_golden_is_certified():
+    """The config-0 objective golden (tests/golden/make_simplex_config0.py): the
+    reference's simplex reached optimality, its own sk_verify certified the point, and
+    an independent simplex (HiGHS) agrees to 1e-12 relative."""
+    here = os.path.join(os.path.dirname(__file__), "golden", "simplex_lp_config0.json")
+    g = json.load(open(here))
+    assert g["status"] == 0 and g["result"] == 0
+    cert = g["sk_verify"]
+    assert max(cert["primal_infeasibility"], cert["dual_infeasibility"], cert["complementarity"]) <= 1e-9
+    assert abs(g["objective"] - g["highs_objective"]) <= 1e-12 * (1 + abs(g["objective"]))
+
+
+def test_pdlp_oracle_reaches_config0_simplex_objective(oracle, instances, golden_dir):
+    """The oracle's restatement of GpuPdlp on the 2,000 x 5,000 LP to 1e-8 relative
+    KKT lands on the reference simplex's objective."""
+    g = json.load(open(os.path.join(golden_dir, "simplex_lp_config0.json")))
+    inst = instances.lp_config0(0)
+    x, y, st = oracle.pdlp(inst, eps=1e-8, max_iterations=400000)
+    assert st["converged"] == 1
+    assert max(st["relative_primal_residual"], st["relative_dual_residual"], st["relative_gap"]) <= 1e-8
+    obj = float(np.dot(inst["c"], x))
+    assert abs(obj - g["objective"]) <= 1e-8 * (1 + abs(g["objective"])), (obj, g["objective"])
+
+
 def test_ruiz_and_pock_chambolle_properties(oracle, instances):
     inst = instances.lp_uniform(5, 80, 200, 4)
     r, c, conv = oracle.ruiz(inst, 100, 1e-2)
