@@ -216,6 +216,28 @@ SANKHYA_CUDA_API int sankhya_b200_pdlp_solve(
     const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
     double* x_out, double* y_out, SankhyaB200PdlpResult* result);
 
+/* The restarted adaptive solve of a convex QP: minimize c'x + x'Q x / 2 subject
+   to the same bounds, with Q given either as a full symmetric CSR of size
+   cols x cols (hessian, made by sankhya_cuda_csr_create) or as its diagonal
+   (quadratic_diagonal, cols entries, finite and >= 0), the two forms of the
+   reference's solve_qp (cuda/src/sankhya_cuda_lp.cu:36-52, 236-238; the CPU
+   loop's c/src/sk_solve.c:908-923). The diagonal is taken exactly in the
+   primal prox, x+ = proj((x - tau (c + A'y)) / (1 + tau q)); a general Q by a
+   gradient step, x+ = proj(x - tau (c + Q x + A'y)), its curvature along each
+   trial move entering the adaptive step's limit. Restarts, primal weight,
+   precision modes and scaling (of A; Q is scaled by the column factors) are
+   those of sankhya_b200_pdlp_solve, and the relative KKT uses the reduced cost
+   c + Q x + A'y and the QP objectives (primal c'x + x'Qx/2, dual with -x'Qx/2).
+   Needs the adaptive step and algorithm ADAPTIVE. No counterpart in the
+   reference's GPU PDLP, which solves LPs only. Both Hessian arguments NULL
+   solves the LP. */
+SANKHYA_CUDA_API int sankhya_b200_pdlp_solve_qp(
+    const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, const double* quadratic_diagonal,
+    const double* c, const double* row_lower, const double* row_upper,
+    const double* col_lower, const double* col_upper,
+    const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
+    double* x_out, double* y_out, SankhyaB200PdlpResult* result);
+
 /* ------------------------------------------------------- batched LPs */
 
 typedef struct SankhyaB200BatchSettings {

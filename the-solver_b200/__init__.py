@@ -32,7 +32,8 @@ REFERENCE_SYMBOLS = (
 )
 EXTENSION_SYMBOLS = (
     "sankhya_b200_set_timing", "sankhya_b200_last_timing", "sankhya_b200_pdhg_loop",
-    "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve", "sankhya_b200_scale_factors",
+    "sankhya_b200_pdlp_default_settings", "sankhya_b200_pdlp_solve", "sankhya_b200_pdlp_solve_qp",
+    "sankhya_b200_scale_factors",
     "sankhya_b200_batch_default_settings", "sankhya_b200_batch_pdhg", "sankhya_b200_shared_batch_pdhg",
     "sankhya_b200_lp_pdhg_device_noalloc", "sankhya_b200_gnn_default_settings", "sankhya_b200_gnn_create",
     "sankhya_b200_gnn_destroy", "sankhya_b200_gnn_parameter_count", "sankhya_b200_gnn_get_parameters",
@@ -188,6 +189,9 @@ def _declare(L):
         L.sankhya_b200_pdlp_solve.argtypes = [P(CSR), dptr, dptr, dptr, dptr, dptr, P(PdlpSettings), dptr,
                                               dptr, dptr, dptr, P(PdlpResult)]
         L.sankhya_b200_scale_factors.argtypes = [P(CSR), C.c_int, C.c_int, C.c_double, dptr, dptr]
+    if hasattr(L, "sankhya_b200_pdlp_solve_qp"):
+        L.sankhya_b200_pdlp_solve_qp.argtypes = [P(CSR), P(CSR), dptr, dptr, dptr, dptr, dptr, dptr,
+                                                 P(PdlpSettings), dptr, dptr, dptr, dptr, P(PdlpResult)]
     if hasattr(L, "sankhya_b200_batch_pdhg"):
         L.sankhya_b200_batch_default_settings.argtypes = [P(BatchSettings)]
         L.sankhya_b200_batch_default_settings.restype = None
@@ -348,6 +352,25 @@ def pdlp_solve(matrix: Matrix, inst, s: PdlpSettings | None = None, x0=None, y0=
     res = PdlpResult()
     rc = L.sankhya_b200_pdlp_solve(C.byref(matrix.handle), _p(c), _p(rl), _p(ru), _p(cl), _p(cu), C.byref(s),
                                    _p(_d(x0)), _p(_d(y0)), _p(x), _p(y), C.byref(res))
+    return rc, x, y, res.as_dict()
+
+
+def pdlp_solve_qp(matrix: Matrix, inst, s: PdlpSettings | None = None, hessian: Matrix | None = None, qdiag=None,
+                  x0=None, y0=None, want_dual=True, **over):
+    """sankhya_b200_pdlp_solve_qp: the restarted solve with x'Q x / 2 in the objective,
+    Q a full symmetric Matrix (hessian) or its diagonal (qdiag)."""
+    L = lib()
+    s = s or pdlp_default_settings()
+    get = lambda k: _d(over[k]) if k in over else _d(inst[k])
+    c, rl, ru, cl, cu = get("c"), get("rl"), get("ru"), get("cl"), get("cu")
+    n, m = matrix.handle.cols, matrix.handle.rows
+    x = np.zeros(n)
+    y = np.zeros(m) if want_dual else None
+    res = PdlpResult()
+    qd = _d(qdiag)
+    rc = L.sankhya_b200_pdlp_solve_qp(C.byref(matrix.handle), C.byref(hessian.handle) if hessian is not None else None,
+                                      _p(qd), _p(c), _p(rl), _p(ru), _p(cl), _p(cu), C.byref(s), _p(_d(x0)),
+                                      _p(_d(y0)), _p(x), _p(y), C.byref(res))
     return rc, x, y, res.as_dict()
 
 

@@ -92,7 +92,8 @@ __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, T* __res
                               const T* __restrict__ x_cand, T* __restrict__ x_sum, T* __restrict__ y,
                               T* __restrict__ y_cand, T* __restrict__ y_sum, T* __restrict__ ax, T* __restrict__ ax_prev,
                               const T* __restrict__ ax_cand, const T* __restrict__ rl, const T* __restrict__ ru,
-                              const double* __restrict__ y_center, int make_candidate) {
+                              const double* __restrict__ y_center, T* __restrict__ qx, const T* __restrict__ qx_cand,
+                              int make_candidate) {
     const bool acc = st->accepted != 0.0;
     const T sigma = static_cast<T>(st->eta * st->omega);
     const int stride = blockDim.x * gridDim.x;
@@ -125,6 +126,7 @@ __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, T* __res
             const T xc = x_cand[j];
             x[j] = xc;
             x_sum[j] += xc;
+            if (qx) qx[j] = qx_cand[j];
         }
     }
 }
@@ -133,7 +135,10 @@ __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, T* __res
 // programming using primal-dual hybrid gradient" (NeurIPS 2021, section 3.1).
 // For a trial move (dx, dy) made with step `used`, PDHG stays stable while the
 // step is at most  |dz|^2_w / (2 |dy' A dx|),  with |dz|^2_w = w |dx|^2 + |dy|^2 / w
-// (w the primal weight). The move is kept when `used` is within that limit. The
+// (w the primal weight). With a quadratic objective taken by a gradient step (a
+// general Hessian Q) the smooth term's curvature along the move adds to the
+// coupling: the limit is |dz|^2_w / (2 |dy' A dx| + dx' Q dx), the local form of the
+// Condat-Vu condition 1/tau - sigma |A|^2 >= |Q| (cross = |dy' A dx| + dx' Q dx / 2). The move is kept when `used` is within that limit. The
 // next step is min((1 - (k+1)^-0.3) limit, (1 + (k+1)^-0.6) used) for the k-th
 // trial: both factors tend to 1, so the step settles just under the limit.
 // With no interaction (or no movement) the limit is the largest allowed step;
@@ -157,27 +162,62 @@ __device__ __forceinline__ StepRule step_rule(double used, double w, double dx2,
     return r;
 }
 
-// K2 (PdlpKernels.cu:391-400 primal candidate + the |dx|^2 part of :405-430)
-template <class T>
+// Quadratic objective of the QP entry point: none (LP), a diagonal Hessian taken
+// exactly in the primal prox, or a general Hessian taken by a gradient step.
+enum QMode { kLp = 0, kQDiag = 1, kQGeneral = 2 };
+
+// K2 (PdlpKernels.cu:391-400 primal candidate + the |dx|^2 part of :405-430). QP:
+// diagonal q: x_cand = proj((x - tau (c + A'y)) / (1 + tau q)) (the prox of
+// c'x + q x^2 / 2 over the box, the reference's sankhya_cuda_lp.cu:36-52 form);
+// general Q: x_cand = proj(x - tau (c + Q x + A'y)), with Q x kept per column.
+template <class T, int QM = kLp>
 struct PrimalCandEpi {
     const PdlpState* st;
     const T* __restrict__ x;
     const T* __restrict__ c;
     const T* __restrict__ cl;
     const T* __restrict__ cu;
+    const T* __restrict__ q;  // QM: the diagonal (kQDiag) or Q x (kQGeneral); unused for LP
     T* __restrict__ x_cand;
     double* __restrict__ partial;
     using Acc = Slots<1, 1u>;
     struct Row {
-        T x, c, lo, hi;
+        T x, c, lo, hi, q;
     };
-    __device__ __forceinline__ Row load(int j) const { return Row{x[j], c[j], cl[j], cu[j]}; }
+    __device__ __forceinline__ Row load(int j) const {
+        return Row{x[j], c[j], cl[j], cu[j], QM == kLp ? T(0) : q[j]};
+    }
     __device__ __forceinline__ void store(int j, T aty, const Row& r, Acc& acc) const {
         const T tau = static_cast<T>(st->eta / st->omega);
-        const T xc = clampf<T>(r.x - tau * (r.c + aty), r.lo, r.hi);
+        T xc;
+        if (QM == kQDiag) xc = clampf<T>((r.x - tau * (r.c + aty)) / (T(1) + tau * r.q), r.lo, r.hi);
+        else if (QM == kQGeneral) xc = clampf<T>(r.x - tau * (r.c + r.q + aty), r.lo, r.hi);
+        else xc = clampf<T>(r.x - tau * (r.c + aty), r.lo, r.hi);
         x_cand[j] = xc;
         const double dx = static_cast<double>(xc) - static_cast<double>(r.x);
         acc.add(0, dx * dx);
+    }
+    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
+};
+
+// K3q (general Hessian): Q x_cand, and the curvature dx' Q dx = dx'(Q x_cand - Q x)
+// of the trial move in block partials, which K3's last block adds to the coupling.
+template <class T>
+struct QProbeEpi {
+    const T* __restrict__ x;
+    const T* __restrict__ x_cand;
+    const T* __restrict__ qx;
+    T* __restrict__ qx_cand;
+    double* __restrict__ partial;
+    using Acc = Slots<1, 1u>;
+    struct Row {
+        T x, xc, qx;
+    };
+    __device__ __forceinline__ Row load(int j) const { return Row{x[j], x_cand[j], qx[j]}; }
+    __device__ __forceinline__ void store(int j, T qxc, const Row& r, Acc& acc) const {
+        qx_cand[j] = qxc;
+        const double dx = static_cast<double>(r.xc) - static_cast<double>(r.x);
+        acc.add(0, dx * (static_cast<double>(qxc) - static_cast<double>(r.qx)));
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
 };
@@ -193,6 +233,8 @@ struct ProbeEpi {
     double* __restrict__ partial;           // this kernel's [gridDim.x * 2]
     const double* __restrict__ partial_dx;  // K2's [grid_dx]
     int grid_dx;
+    const double* __restrict__ partial_q;   // K3q's [grid_q] curvature partials, or null
+    int grid_q;
     using Acc = Slots<2, 3u>;
     struct Row {
         T y, yc, ax;
@@ -216,28 +258,34 @@ struct ProbeEpi {
         if (!last) return;
         __threadfence();
         // fixed-order combine: thread k sums a strided slice, then a fixed tree
-        __shared__ double red[3][kThreads];
-        double a = 0.0, b = 0.0, d = 0.0;
+        __shared__ double red[4][kThreads];
+        double a = 0.0, b = 0.0, d = 0.0, e = 0.0;
         for (int g = threadIdx.x; g < grid_dx; g += kThreads) a += __ldcg(partial_dx + g);
         for (int g = threadIdx.x; g < static_cast<int>(gridDim.x); g += kThreads) {
             b += __ldcg(partial + 2 * g);
             d += __ldcg(partial + 2 * g + 1);
         }
+        if (partial_q)
+            for (int g = threadIdx.x; g < grid_q; g += kThreads) e += __ldcg(partial_q + g);
         red[0][threadIdx.x] = a;
         red[1][threadIdx.x] = b;
         red[2][threadIdx.x] = d;
+        red[3][threadIdx.x] = e;
         __syncthreads();
         for (int s = kThreads / 2; s > 0; s >>= 1) {
             if (threadIdx.x < s) {
                 red[0][threadIdx.x] += red[0][threadIdx.x + s];
                 red[1][threadIdx.x] += red[1][threadIdx.x + s];
                 red[2][threadIdx.x] += red[2][threadIdx.x + s];
+                red[3][threadIdx.x] += red[3][threadIdx.x + s];
             }
             __syncthreads();
         }
         if (threadIdx.x != 0) return;
         const double probe = st->updates + 1.0;
-        const StepRule rule = step_rule(st->eta, st->omega, red[0][0], red[1][0], fabs(red[2][0]), probe,
+        double cross = fabs(red[2][0]);
+        if (partial_q) cross += 0.5 * fmax(red[3][0], 0.0);
+        const StepRule rule = step_rule(st->eta, st->omega, red[0][0], red[1][0], cross, probe,
                                         st->eta_min, st->eta_max);
         st->dx_sq = red[0][0];
         st->dy_sq = red[1][0];
@@ -440,21 +488,31 @@ struct ResRowsEpi {
 // 3 |x|^2, 4 |x - x_restart|^2 (sums), 5 max |x - proj(x - (c + A'y))| (max;
 // the column KKT residual, which sees reduced costs of interior variables even
 // when every bound is finite and the dual violation itself is zero).
-template <class T>
+// QP (QM != kLp): the reduced cost is c + Q x + A'y, slot 2 takes c'x + x'Q x / 2
+// and slot 1 the dual objective's -x'Q x / 2 (the QP's Wolfe dual); q is the
+// diagonal (kQDiag) or Q x of the evaluated point (kQGeneral).
+template <class T, int QM = kLp>
 struct ResColsEpi {
     const T* __restrict__ x;
     const T* __restrict__ x_restart;
     const T* __restrict__ c;
     const T* __restrict__ cl;
     const T* __restrict__ cu;
+    const T* __restrict__ q;
     T* __restrict__ aty_out;  // may be null
     double* __restrict__ partial;
     using Acc = Slots<6, 0x1Fu>;
     __device__ __forceinline__ void row(int j, T atyt, Acc& acc) const {
         if (aty_out) aty_out[j] = atyt;
         const double xj = x[j], lo = cl[j], hi = cu[j], cj = c[j];
-        const double r = cj + static_cast<double>(atyt);
-        acc.add(2, cj * xj);
+        double r = cj + static_cast<double>(atyt);
+        double half_xqx = 0.0;
+        if (QM != kLp) {
+            const double qxj = QM == kQDiag ? static_cast<double>(q[j]) * xj : static_cast<double>(q[j]);
+            r = cj + qxj + static_cast<double>(atyt);
+            half_xqx = 0.5 * xj * qxj;
+        }
+        acc.add(2, QM == kLp ? cj * xj : cj * xj + half_xqx);
         acc.add(3, xj * xj);
         const double dx = xj - static_cast<double>(x_restart[j]);
         acc.add(4, dx * dx);
@@ -472,7 +530,7 @@ struct ResColsEpi {
             viol = fabs(r);
         }
         acc.add(0, viol * viol);
-        acc.add(1, term);
+        acc.add(1, QM == kLp ? term : term - half_xqx);
         acc.max(5, fabs(xj - fmin(fmax(xj - r, lo), hi)));
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
@@ -510,7 +568,10 @@ struct ResRowsCenteredEpi {
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
 };
 
-template <class T>
+// QP: rc_center includes Q x_center; the deviation's part is q dx (diagonal, FP64
+// q) or Q dx (general, the FP32 product dq), and Q x of the combined point is
+// q x (diagonal) or qx_center + dq (general).
+template <class T, int QM = kLp>
 struct ResColsCenteredEpi {
     const T* __restrict__ dx;
     const double* __restrict__ x_center;
@@ -518,13 +579,24 @@ struct ResColsCenteredEpi {
     const double* __restrict__ c;
     const double* __restrict__ cl;
     const double* __restrict__ cu;
+    const double* __restrict__ q64;      // kQDiag: the FP64 diagonal; kQGeneral: Q x_center
+    const T* __restrict__ dq;            // kQGeneral: Q dx of the evaluated deviation
     double* __restrict__ partial;
     using Acc = Slots<6, 0x1Fu>;
     __device__ __forceinline__ void row(int j, T atdy, Acc& acc) const {
         const double d = static_cast<double>(dx[j]);
         const double xj = x_center[j] + d, lo = cl[j], hi = cu[j], cj = c[j];
-        const double r = rc_center[j] + static_cast<double>(atdy);
-        acc.add(2, cj * xj);
+        double r = rc_center[j] + static_cast<double>(atdy);
+        double half_xqx = 0.0;
+        if (QM == kQDiag) {
+            r += q64[j] * d;
+            half_xqx = 0.5 * xj * (q64[j] * xj);
+        } else if (QM == kQGeneral) {
+            const double g = static_cast<double>(dq[j]);
+            r += g;
+            half_xqx = 0.5 * xj * (q64[j] + g);
+        }
+        acc.add(2, cj * xj + half_xqx);
         acc.add(3, xj * xj);
         acc.add(4, d * d);
         const bool lf = isfinite(lo), hf = isfinite(hi);
@@ -541,7 +613,7 @@ struct ResColsCenteredEpi {
             viol = fabs(r);
         }
         acc.add(0, viol * viol);
-        acc.add(1, term);
+        acc.add(1, term - half_xqx);
         acc.max(5, fabs(xj - fmin(fmax(xj - r, lo), hi)));
     }
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
@@ -561,14 +633,18 @@ __global__ void k_recenter(int n, int m, const T* __restrict__ from_x, const T* 
 
 // FP32 data of the problem around the center (FP64 in, one rounding out):
 // c + A'yc, column bounds minus xc, row bounds minus A xc; infinite bounds stay infinite.
+// QP: the gradient at the center also holds q x_center (qdiag) or Q x_center (qx_c).
 __global__ void k_frame(int n, int m, const double* __restrict__ c, const double* __restrict__ aty_c,
                         const double* __restrict__ cl, const double* __restrict__ cu, const double* __restrict__ xc,
                         const double* __restrict__ rl, const double* __restrict__ ru, const double* __restrict__ ax_c,
+                        const double* __restrict__ qdiag, const double* __restrict__ qx_c,
                         double* __restrict__ rc_c, float* __restrict__ c32, float* __restrict__ cl32,
                         float* __restrict__ cu32, float* __restrict__ rl32, float* __restrict__ ru32) {
     const int stride = blockDim.x * gridDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
-        const double r = c[j] + aty_c[j];
+        double r = c[j] + aty_c[j];
+        if (qdiag) r += qdiag[j] * xc[j];
+        else if (qx_c) r += qx_c[j];
         rc_c[j] = r;
         c32[j] = static_cast<float>(r);
         cl32[j] = static_cast<float>(cl[j] - xc[j]);
@@ -584,9 +660,13 @@ __global__ void k_frame(int n, int m, const double* __restrict__ c, const double
 // accepted-step count at the restart is recorded as k_restart does.
 template <class T>
 __global__ void k_zero_deviation(int n, int m, T* __restrict__ x, T* __restrict__ x_sum, T* __restrict__ y,
-                                 T* __restrict__ y_sum, T* __restrict__ ax, T* __restrict__ ax_prev, PdlpState* st) {
+                                 T* __restrict__ y_sum, T* __restrict__ ax, T* __restrict__ ax_prev, T* __restrict__ qx,
+                                 PdlpState* st) {
     const int stride = blockDim.x * gridDim.x;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) x[j] = x_sum[j] = T(0);
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        x[j] = x_sum[j] = T(0);
+        if (qx) qx[j] = T(0);
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y[i] = y_sum[i] = ax[i] = ax_prev[i] = T(0);
     if (blockIdx.x == 0 && threadIdx.x == 0) st->accepted_at_restart = st->accept_count;
 }
@@ -654,11 +734,15 @@ __global__ void k_restart(int n, int m, int to_average, int adaptive, T* __restr
                           T* __restrict__ x_bar, const T* __restrict__ x_avg, const T* __restrict__ y_avg,
                           T* __restrict__ ax, T* __restrict__ ax_prev, const T* __restrict__ ax_avg,
                           T* __restrict__ x_sum, T* __restrict__ y_sum, T* __restrict__ x_restart,
-                          T* __restrict__ y_restart, PdlpState* st) {
+                          T* __restrict__ y_restart, T* __restrict__ qx, const T* __restrict__ qx_avg, PdlpState* st) {
     const int stride = blockDim.x * gridDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
         T xj = x[j];
-        if (to_average) { xj = x_avg[j]; x[j] = xj; }
+        if (to_average) {
+            xj = x_avg[j];
+            x[j] = xj;
+            if (qx) qx[j] = qx_avg[j];
+        }
         x_bar[j] = xj;
         x_sum[j] = T(0);
         x_restart[j] = xj;
@@ -1060,10 +1144,13 @@ struct LoopParams {
 // point), its products and the FP32 frame data the iterations run on.
 struct Centered {
     TileCsr A, AT;  // scaled FP64 matrix
+    TileCsr Q;      // scaled FP64 Hessian (QP, general path; ntiles 0 otherwise)
     const double *c = nullptr, *cl = nullptr, *cu = nullptr, *rl = nullptr, *ru = nullptr;
+    const double* qdiag = nullptr;  // scaled FP64 Hessian diagonal (QP, diagonal path)
     double *xc = nullptr, *yc = nullptr, *ax_c = nullptr, *aty_c = nullptr, *rc_c = nullptr;
+    double* qx_c = nullptr;         // Q x_center (general path)
     float *c32 = nullptr, *cl32 = nullptr, *cu32 = nullptr, *rl32 = nullptr, *ru32 = nullptr;
-    int grid_a = 1, grid_at = 1;
+    int grid_a = 1, grid_at = 1, grid_q = 1;
 };
 
 struct LoopStats {
@@ -1093,6 +1180,16 @@ struct Core {
     int grid_rrc = 1, grid_rcc = 1;
     int launches = 0;
     std::vector<cudaGraphExec_t> graphs;
+    // Quadratic objective (the QP entry point): qmode kQDiag with the diagonal qd,
+    // or kQGeneral with the Hessian Q, whose products Q x (committed point),
+    // Q x_cand and Q x_avg ride along like the A-side ones; kLp otherwise.
+    int qmode = kLp;
+    const T* qd = nullptr;
+    TileCsrT<T> Q;
+    DevBuf qblob;
+    T *qx = nullptr, *qx_cand = nullptr, *qx_avg = nullptr;
+    double* part_e = nullptr;
+    int grid_q = 1, grid_qs = 1;
     // Centered mode (FP32 iterations of the FP32_REFINE precision): x, y, ax and the
     // sums are deviations from ctr's FP64 center; the center moves to the restart
     // point at every restart (one refinement), and the window-end residuals are
@@ -1138,10 +1235,14 @@ struct Core {
         A = a;
         AT = at;
         c = c_; cl = cl_; cu = cu_; rl = rl_; ru = ru_;
-        grid_k2 = tiled_grid<PrimalCandEpi<T>, T>(AT);
+        grid_k2 = qmode == kQDiag ? tiled_grid<PrimalCandEpi<T, kQDiag>, T>(AT)
+                  : qmode == kQGeneral ? tiled_grid<PrimalCandEpi<T, kQGeneral>, T>(AT)
+                                       : tiled_grid<PrimalCandEpi<T>, T>(AT);
         grid_k3 = tiled_grid<ProbeEpi<T>, T>(A);
         grid_rr = tiled_grid<ResRowsEpi<T>, T>(A);
-        grid_rc = tiled_grid<ResColsEpi<T>, T>(AT);
+        grid_rc = qmode == kQDiag ? tiled_grid<ResColsEpi<T, kQDiag>, T>(AT)
+                  : qmode == kQGeneral ? tiled_grid<ResColsEpi<T, kQGeneral>, T>(AT)
+                                       : tiled_grid<ResColsEpi<T>, T>(AT);
         grid_df = tiled_grid<DualFixedEpi<T>, T>(A);
         grid_pf = tiled_grid<PrimalFixedEpi<T>, T>(AT);
         grid_ph = tiled_grid<PrimalHalpernEpi<T>, T>(AT);
@@ -1149,39 +1250,96 @@ struct Core {
         grid_pt = tiled_grid<PrimalTEpi<T>, T>(AT);
         grid_dt = tiled_grid<DualTEpi<T>, T>(A);
         grid_rrc = tiled_grid<ResRowsCenteredEpi<T>, T>(A);
-        grid_rcc = tiled_grid<ResColsCenteredEpi<T>, T>(AT);
+        grid_rcc = qmode == kQDiag ? tiled_grid<ResColsCenteredEpi<T, kQDiag>, T>(AT)
+                   : qmode == kQGeneral ? tiled_grid<ResColsCenteredEpi<T, kQGeneral>, T>(AT)
+                                        : tiled_grid<ResColsCenteredEpi<T>, T>(AT);
         for (auto g : graphs)
             if (g) cudaGraphExecDestroy(g);
         graphs.clear();
     }
 
-    // Residual sums of (xv, yv) into out[0..13]; ax_out / aty_out optional.
-    void residuals(const T* xv, const T* yv, T* ax_out, T* aty_out, double* out, int clear_accept) {
-        if (ctr) {
-            const int nbr = A.ntiles ? grid_rrc : 0, nbc = AT.ntiles ? grid_rcc : 0;
-            launch_tiled(A, xv, ResRowsCenteredEpi<T>{yv, ctr->yc, ctr->ax_c, ctr->rl, ctr->ru, ax_out, part_a},
-                         stream, grid_rrc);
-            launch_tiled(AT, yv, ResColsCenteredEpi<T>{xv, ctr->xc, ctr->rc_c, ctr->c, ctr->cl, ctr->cu, part_b},
-                         stream, grid_rcc);
-            k_res_combine<<<1, kThreads, 0, stream>>>(part_a, nbr, part_b, nbc, out, st, clear_accept);
-            launches += 3;
-            return;
+    // The QP's Hessian: a diagonal (diag) or a general matrix (q, n x n); call after
+    // allocate and before set_problem. The general path owns Q x, Q x_cand, Q x_avg
+    // and the curvature partials.
+    int set_hessian(const T* diag, const TileCsrT<T>* q) {
+        if (diag) {
+            qmode = kQDiag;
+            qd = diag;
+            return 0;
         }
+        if (!q) return 0;
+        qmode = kQGeneral;
+        Q = *q;
+        const size_t nb = (static_cast<size_t>(n) * sizeof(T) + 255) / 256 * 256;
+        const size_t pb = (static_cast<size_t>(sms) * 8 * 8 * 8 + 255) / 256 * 256;
+        if (qblob.alloc(3 * nb + pb, "cudaMalloc Hessian products")) return -1;
+        qx = qblob.as<T>();
+        qx_cand = reinterpret_cast<T*>(qblob.as<char>() + nb);
+        qx_avg = reinterpret_cast<T*>(qblob.as<char>() + 2 * nb);
+        part_e = reinterpret_cast<double*>(qblob.as<char>() + 3 * nb);
+        grid_q = tiled_grid<QProbeEpi<T>, T>(Q);
+        grid_qs = tiled_grid<StoreEpiT<T>, T>(Q);
+        return 0;
+    }
+
+    template <int QM>
+    void residuals_q(const T* xv, const T* yv, T* ax_out, T* aty_out, const T* qv, double* out, int clear_accept) {
         const int nbr = A.ntiles ? grid_rr : 0, nbc = AT.ntiles ? grid_rc : 0;
         launch_tiled(A, xv, ResRowsEpi<T>{yv, y_restart, rl, ru, ax_out, part_a}, stream, grid_rr);
-        launch_tiled(AT, yv, ResColsEpi<T>{xv, x_restart, c, cl, cu, aty_out, part_b}, stream, grid_rc);
+        launch_tiled(AT, yv, ResColsEpi<T, QM>{xv, x_restart, c, cl, cu, qv, aty_out, part_b}, stream, grid_rc);
         k_res_combine<<<1, kThreads, 0, stream>>>(part_a, nbr, part_b, nbc, out, st, clear_accept);
         launches += 3;
     }
 
+    template <int QM>
+    void residuals_centered(const T* xv, const T* yv, T* ax_out, const T* dq, double* out, int clear_accept) {
+        const int nbr = A.ntiles ? grid_rrc : 0, nbc = AT.ntiles ? grid_rcc : 0;
+        launch_tiled(A, xv, ResRowsCenteredEpi<T>{yv, ctr->yc, ctr->ax_c, ctr->rl, ctr->ru, ax_out, part_a}, stream,
+                     grid_rrc);
+        const double* q64 = QM == kQDiag ? ctr->qdiag : ctr->qx_c;
+        launch_tiled(AT, yv, ResColsCenteredEpi<T, QM>{xv, ctr->xc, ctr->rc_c, ctr->c, ctr->cl, ctr->cu, q64, dq,
+                                                       part_b},
+                     stream, grid_rcc);
+        k_res_combine<<<1, kThreads, 0, stream>>>(part_a, nbr, part_b, nbc, out, st, clear_accept);
+        launches += 3;
+    }
+
+    // Residual sums of (xv, yv) into out[0..13]; ax_out / aty_out optional; qv is
+    // Q xv (general Hessian) of the evaluated point.
+    void residuals(const T* xv, const T* yv, T* ax_out, T* aty_out, double* out, int clear_accept,
+                   const T* qv = nullptr) {
+        if (ctr) {
+            if (qmode == kQDiag) residuals_centered<kQDiag>(xv, yv, ax_out, nullptr, out, clear_accept);
+            else if (qmode == kQGeneral) residuals_centered<kQGeneral>(xv, yv, ax_out, qv, out, clear_accept);
+            else residuals_centered<kLp>(xv, yv, ax_out, nullptr, out, clear_accept);
+            return;
+        }
+        if (qmode == kQDiag) residuals_q<kQDiag>(xv, yv, ax_out, aty_out, qd, out, clear_accept);
+        else if (qmode == kQGeneral) residuals_q<kQGeneral>(xv, yv, ax_out, aty_out, qv, out, clear_accept);
+        else residuals_q<kLp>(xv, yv, ax_out, aty_out, nullptr, out, clear_accept);
+    }
+
     void adaptive_iteration(bool make_candidate) {
+        const bool general = qmode == kQGeneral;
         k_commit_dual<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, x, x_cand, x_sum, y, y_cand, y_sum,
                                                                       ax, ax_prev, ax_cand, rl, ru,
-                                                                      ctr ? ctr->yc : nullptr, make_candidate ? 1 : 0);
+                                                                      ctr ? ctr->yc : nullptr, general ? qx : nullptr,
+                                                                      qx_cand, make_candidate ? 1 : 0);
         ++launches;
         if (!make_candidate) return;
-        launch_tiled(AT, y_cand, PrimalCandEpi<T>{st, x, c, cl, cu, x_cand, part_c}, stream, grid_k2);
-        launch_tiled(A, x_cand, ProbeEpi<T>{st, y, y_cand, ax, ax_cand, part_d, part_c, AT.ntiles ? grid_k2 : 0},
+        if (qmode == kQDiag)
+            launch_tiled(AT, y_cand, PrimalCandEpi<T, kQDiag>{st, x, c, cl, cu, qd, x_cand, part_c}, stream, grid_k2);
+        else if (general)
+            launch_tiled(AT, y_cand, PrimalCandEpi<T, kQGeneral>{st, x, c, cl, cu, qx, x_cand, part_c}, stream,
+                         grid_k2);
+        else
+            launch_tiled(AT, y_cand, PrimalCandEpi<T>{st, x, c, cl, cu, nullptr, x_cand, part_c}, stream, grid_k2);
+        if (general) {
+            launch_tiled(Q, x_cand, QProbeEpi<T>{x, x_cand, qx, qx_cand, part_e}, stream, grid_q);
+            ++launches;
+        }
+        launch_tiled(A, x_cand, ProbeEpi<T>{st, y, y_cand, ax, ax_cand, part_d, part_c, AT.ntiles ? grid_k2 : 0,
+                                            general ? part_e : nullptr, Q.ntiles ? grid_q : 0},
                      stream, grid_k3);
         launches += 2;
     }
@@ -1205,10 +1363,14 @@ struct Core {
                 else fixed_iteration(static_cast<T>(tau), static_cast<T>(sigma));
             }
             if (adaptive) adaptive_iteration(false);  // commit the last probe
-            residuals(x, y, nullptr, nullptr, res, 0);
+            residuals(x, y, nullptr, nullptr, res, 0, qx);
             k_average<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, st, adaptive ? 1 : 0, x_sum, y_sum, x_avg,
                                                                        y_avg);
-            residuals(x_avg, y_avg, ax_avg, nullptr, res + 16, 1);
+            if (qmode == kQGeneral) {
+                launch_tiled(Q, x_avg, StoreEpiT<T>{qx_avg}, stream, grid_qs);
+                ++launches;
+            }
+            residuals(x_avg, y_avg, ax_avg, nullptr, res + 16, 1, qx_avg);
             cudaMemcpyAsync(host, res, 32 * sizeof(double), cudaMemcpyDeviceToHost, stream);
             B200_TRY(cudaStreamEndCapture(stream, &g), "end capture");
             cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
@@ -1231,8 +1393,15 @@ struct Core {
     void build_frame() {
         launch_tiled(ctr->A, ctr->xc, StoreEpi{ctr->ax_c}, stream, ctr->grid_a);
         launch_tiled(ctr->AT, ctr->yc, StoreEpi{ctr->aty_c}, stream, ctr->grid_at);
+        const bool general = qmode == kQGeneral;
+        if (general) {
+            launch_tiled(ctr->Q, ctr->xc, StoreEpi{ctr->qx_c}, stream, ctr->grid_q);
+            ++launches;
+        }
         k_frame<<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, ctr->c, ctr->aty_c, ctr->cl, ctr->cu, ctr->xc,
-                                                             ctr->rl, ctr->ru, ctr->ax_c, ctr->rc_c, ctr->c32,
+                                                             ctr->rl, ctr->ru, ctr->ax_c,
+                                                             qmode == kQDiag ? ctr->qdiag : nullptr,
+                                                             general ? ctr->qx_c : nullptr, ctr->rc_c, ctr->c32,
                                                              ctr->cl32, ctr->cu32, ctr->rl32, ctr->ru32);
         launches += 3;
         ++recenters;
@@ -1246,7 +1415,8 @@ struct Core {
         ++launches;
         if (!rebuild) return;
         build_frame();
-        k_zero_deviation<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, x, x_sum, y, y_sum, ax, ax_prev, st);
+        k_zero_deviation<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(n, m, x, x_sum, y, y_sum, ax, ax_prev,
+                                                                          qmode == kQGeneral ? qx : nullptr, st);
         ++launches;
     }
 
@@ -1389,6 +1559,7 @@ struct Core {
         B200_TRY(cudaMemcpyAsync(x_bar, x, nb, cudaMemcpyDeviceToDevice, stream), "copy");
         B200_TRY(cudaMemcpyAsync(y_restart, y, mb, cudaMemcpyDeviceToDevice, stream), "copy");
         if (m) launch_tiled(A, x, StoreEpiT<T>{ax}, stream, tiled_grid<StoreEpiT<T>, T>(A));
+        if (qmode == kQGeneral) launch_tiled(Q, x, StoreEpiT<T>{qx}, stream, grid_qs);
         B200_TRY(cudaMemcpyAsync(ax_prev, ax, mb, cudaMemcpyDeviceToDevice, stream), "copy");
         const double eta_global = kStepSafety / lp.matrix_norm;
         const double eta_min = lp.eta_min_factor / lp.matrix_norm, eta_max = lp.eta_max_factor / lp.matrix_norm;
@@ -1473,7 +1644,7 @@ struct Core {
             } else {
                 k_restart<T><<<eg(std::max(n, m)), kThreads, 0, stream>>>(
                     n, m, average_better ? 1 : 0, lp.adaptive ? 1 : 0, x, y, x_bar, x_avg, y_avg, ax, ax_prev,
-                    ax_avg, x_sum, y_sum, x_restart, y_restart, st);
+                    ax_avg, x_sum, y_sum, x_restart, y_restart, qmode == kQGeneral ? qx : nullptr, qx_avg, st);
                 ++launches;
             }
             windows_since_restart = 0;
@@ -1524,10 +1695,21 @@ extern "C" void sankhya_b200_pdlp_default_settings(SankhyaB200PdlpSettings* s) {
     s->ruiz_tolerance = 1e-2;
 }
 
-extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const double* c, const double* row_lower,
-                                       const double* row_upper, const double* col_lower, const double* col_upper,
-                                       const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
-                                       double* x_out, double* y_out, SankhyaB200PdlpResult* result) {
+namespace b200 {
+namespace {
+
+__global__ void k_scale_diag(int n, const double* __restrict__ q, const double* __restrict__ Cs,
+                             double* __restrict__ out) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += blockDim.x * gridDim.x)
+        out[j] = (q[j] * Cs[j]) * Cs[j];
+}
+
+// The LP and QP solve: minimize c'x (+ x'Q x / 2) over rl <= A x <= ru, cl <= x <= cu,
+// with Q a general symmetric Hessian (hessian, full CSR) or a diagonal (qdiag).
+int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, const double* qdiag, const double* c,
+               const double* row_lower, const double* row_upper, const double* col_lower, const double* col_upper,
+               const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0, double* x_out,
+               double* y_out, SankhyaB200PdlpResult* result) {
     clear_error();
     (void)cudaGetLastError();  // a caller's earlier non-sticky error is not ours
     if (!result) return fail_msg("null result");
@@ -1560,6 +1742,14 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         s.ruiz_iterations < 0 || (s.precision != SANKHYA_B200_FP64 && s.precision != SANKHYA_B200_FP32_REFINE))
         return fail_msg("invalid PDLP settings");
     const int n = matrix->cols, m = matrix->rows;
+    const bool quadratic = hessian != nullptr || qdiag != nullptr;
+    if (hessian && qdiag) return fail_msg("give either a Hessian or its diagonal, not both");
+    if (hessian && (hessian->rows != n || hessian->cols != n)) return fail_msg("the Hessian must be cols x cols");
+    if (qdiag)
+        for (int j = 0; j < n; ++j)
+            if (!std::isfinite(qdiag[j]) || qdiag[j] < 0.0) return fail_msg("invalid quadratic diagonal");
+    if (quadratic && (s.algorithm != SANKHYA_B200_PDLP_ADAPTIVE || !s.adaptive_step))
+        return fail_msg("the QP solve runs the adaptive step of the restarted loop");
     for (int j = 0; j < n; ++j)
         if (!std::isfinite(c[j]) || std::isnan(col_lower[j]) || std::isnan(col_upper[j]) || col_lower[j] > col_upper[j])
             return fail_msg("invalid cost or column bound");
@@ -1614,11 +1804,33 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     int refinements = 0;
     int launches = sc.launches;
 
+    // QP: the Hessian in the scaled space, Q' = C Q C (a diagonal q' = C^2 q)
+    std::shared_ptr<Plan> qplan;
+    DevBuf qbuf;
+    TileCsr Qs;
+    double* qd_s = nullptr;
+    if (hessian) {
+        if (get_plan(hessian, &qplan)) return -1;
+        if (qbuf.alloc(static_cast<size_t>(qplan->a.nnz) * 8 + 256, "cudaMalloc scaled Hessian")) return -1;
+        Qs = qplan->a;
+        Qs.val = qbuf.as<double>();
+        k_scale_values<<<std::min((n + 7) / 8 + 1, sc.sms * 16), kThreads, 0, stream>>>(
+            n, qplan->a.ptr, qplan->a.idx, qplan->a.val, sc.Cs, sc.Cs, 0, qbuf.as<double>());
+        ++launches;
+    } else if (qdiag) {
+        if (qbuf.alloc(static_cast<size_t>(n) * 8 + 256, "cudaMalloc scaled Hessian diagonal")) return -1;
+        qd_s = qbuf.as<double>();
+        if (n) B200_TRY(cudaMemcpyAsync(qd_s, qdiag, nb, cudaMemcpyHostToDevice, stream), "upload diagonal");
+        k_scale_diag<<<eg(n), kThreads, 0, stream>>>(n, qd_s, sc.Cs, qd_s);
+        ++launches;
+    }
+
     // FP64 point of the scaled problem (x^, y^): starts at zeros or the warm start
     Core<double> hi;
     hi.stream = stream;
     hi.host = hs.p;
     if (hi.allocate(n, m, sc.sms)) return -1;
+    if (hi.set_hessian(qd_s, hessian ? &Qs : nullptr)) return -1;
     hi.set_problem(sc.A, sc.AT, sc.c, sc.cl, sc.cu, sc.rl, sc.ru);
     B200_TRY(cudaMemsetAsync(hi.x, 0, std::max<size_t>(nb, 1), stream), "zero");
     B200_TRY(cudaMemsetAsync(hi.y, 0, std::max<size_t>(mb, 1), stream), "zero");
@@ -1647,7 +1859,7 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         const size_t nd = (static_cast<size_t>(n) * 8 + 255) / 256 * 256;
         const size_t md = (static_cast<size_t>(m) * 8 + 255) / 256 * 256;
         if (blob32.alloc(3 * nf + 2 * mf + 256, "cudaMalloc FP32 frame")) return -1;
-        if (cbuf.alloc(2 * nd + md + 256, "cudaMalloc FP64 center products")) return -1;
+        if (cbuf.alloc(3 * nd + md + 256, "cudaMalloc FP64 center products")) return -1;
         char* base = blob32.as<char>();
         Centered ctr;
         ctr.A = sc.A;
@@ -1665,10 +1877,30 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
         ctr.ru32 = reinterpret_cast<float*>(base + 3 * nf + mf);
         ctr.grid_a = tiled_grid<StoreEpi>(sc.A);
         ctr.grid_at = tiled_grid<StoreEpi>(sc.AT);
+        // QP: the FP64 Hessian for the center's gradient and residuals, FP32 copies for
+        // the deviations' products
+        DevBuf q32buf;
+        TileCsrT<float> Q32;
+        float* qd32 = nullptr;
+        ctr.qdiag = qd_s;
+        if (hessian) {
+            ctr.Q = Qs;
+            ctr.qx_c = reinterpret_cast<double*>(cbuf.as<char>() + 2 * nd + md);
+            ctr.grid_q = tiled_grid<StoreEpi>(Qs);
+            const size_t qnnz = static_cast<size_t>(Qs.nnz);
+            if (q32buf.alloc(qnnz * 4 + 256, "cudaMalloc FP32 Hessian")) return -1;
+            k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(qnnz), Qs.val, q32buf.as<float>());
+            Q32 = Qs.with_values<float>(q32buf.as<float>());
+        } else if (qdiag) {
+            if (q32buf.alloc(static_cast<size_t>(n) * 4 + 256, "cudaMalloc FP32 Hessian diagonal")) return -1;
+            qd32 = q32buf.as<float>();
+            k_narrow<<<eg(n), kThreads, 0, stream>>>(n, qd_s, qd32);
+        }
         Core<float> lo;
         lo.stream = stream;
         lo.host = hs.p;
         if (lo.allocate(n, m, sc.sms)) return -1;
+        if (lo.set_hessian(qd32, hessian ? &Q32 : nullptr)) return -1;
         lo.set_problem(sc.A.with_values<float>(a32), sc.AT.with_values<float>(at32), ctr.c32, ctr.cl32, ctr.cu32,
                        ctr.rl32, ctr.ru32);
         lo.ctr = &ctr;
@@ -1774,6 +2006,26 @@ extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const doubl
     ts.last.checkpoints = syncs;
     ts.last.kernel_launches = launches;
     return stats.numeric ? -2 : 0;
+}
+
+}  // namespace
+}  // namespace b200
+
+extern "C" int sankhya_b200_pdlp_solve(const SankhyaCudaCSR* matrix, const double* c, const double* row_lower,
+                                       const double* row_upper, const double* col_lower, const double* col_upper,
+                                       const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
+                                       double* x_out, double* y_out, SankhyaB200PdlpResult* result) {
+    return b200::pdlp_solve(matrix, nullptr, nullptr, c, row_lower, row_upper, col_lower, col_upper, settings, x0,
+                            y0, x_out, y_out, result);
+}
+
+extern "C" int sankhya_b200_pdlp_solve_qp(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian,
+                                          const double* quadratic_diagonal, const double* c, const double* row_lower,
+                                          const double* row_upper, const double* col_lower, const double* col_upper,
+                                          const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
+                                          double* x_out, double* y_out, SankhyaB200PdlpResult* result) {
+    return b200::pdlp_solve(matrix, hessian, quadratic_diagonal, c, row_lower, row_upper, col_lower, col_upper,
+                            settings, x0, y0, x_out, y_out, result);
 }
 
 extern "C" int sankhya_b200_scale_factors(const SankhyaCudaCSR* matrix, int scaling, int ruiz_iterations,
