@@ -571,7 +571,9 @@ def run_qp(args):
     entries per column), bounds [-5, 5], rows x0 -/+ U(0,1). Device time per PDHG
     iteration of the diagonal-proximal path (sankhya_cuda_diagonal_qp_pdhg, Q's
     diagonal D) and of the general sparse-Hessian path (sankhya_cuda_sparse_qp_pdhg,
-    explicit Q = D + L L^T: one more fused product per iteration). Prints one JSON line."""
+    explicit Q = D + L L^T: one more fused product per iteration), then the restarted
+    PDLP QP solve (sankhya_b200_pdlp_solve_qp) to 1e-6 relative KKT on both paths, FP64
+    and FP32 iterations refined in FP64. Prints one JSON line."""
     E = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
     I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
     inst = I.qp_config2(2)
@@ -603,6 +605,26 @@ def run_qp(args):
         out[name] = {"us_per_iteration": round(best, 2), "algorithmic_bytes": byt,
                      "algorithmic_gbs": round(byt / best / 1e3, 1), "frac_of_hbm": round(byt / best / 1e3 / peak, 3),
                      "objective_after": r["objective"]}
+    # restarted PDLP with the quadratic term to 1e-6 relative KKT: the diagonal Hessian
+    # (exact prox; the QP with Q's diagonal D) and the general Hessian (Q = D + L L^T,
+    # one more fused product per iteration), FP64 and FP32 iterations refined in FP64
+    ttk = {"eps": 1e-6, "relative_kkt": "max(primal, dual, gap), reduced cost c + Qx + A'y"}
+    for name, kw in (("diagonal", dict(qdiag=inst["qdiag"])), ("sparse_hessian", dict(hessian=Q))):
+        for label, prec in (("fp64", E.FP64), ("fp32_refined", E.FP32_REFINE)):
+            ps_ = E.pdlp_default_settings()
+            ps_.eps_optimal, ps_.precision, ps_.time_limit, ps_.max_iterations = 1e-6, prec, 120.0, 20_000_000
+            t0 = time.perf_counter()
+            rc, x, y, r = E.pdlp_solve_qp(A, inst, ps_, **kw)
+            wall = time.perf_counter() - t0
+            ttk[f"{name}_{label}"] = {"seconds": round(wall, 3), "status": r["status"], "iterations": r["iterations"],
+                                      "restarts": r["restarts"], "refinements": r["refinements"],
+                                      "primal_objective": _finite(r["primal_objective"]),
+                                      "kkt": [_finite(r[k]) for k in ("relative_primal_residual",
+                                                                      "relative_dual_residual", "relative_gap")]}
+        a, b_ = ttk[f"{name}_fp64"], ttk[f"{name}_fp32_refined"]
+        if a["status"] == 0 and b_["status"] == 0 and b_["seconds"] > 0:
+            ttk[f"{name}_speedup_fp32_refined_vs_fp64"] = round(a["seconds"] / b_["seconds"], 3)
+    out["time_to_kkt"] = ttk
     print(json.dumps(out))
     return 0
 
