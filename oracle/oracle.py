@@ -412,6 +412,8 @@ def build_sk_model(keep: _Keep, inst, quadratic=False):
     for k, f in (("c", "c"), ("rl", "rlow"), ("ru", "rupp"), ("cl", "clow"), ("cu", "cupp")):
         setattr(model, f, _p(keep.d(inst[k])))
     vt = np.zeros(max(n, 1), dtype=np.uint8)
+    if "vartype" in inst:   # SK_INTEGER (1) marks the integer columns of a MILP
+        vt[:n] = np.asarray(inst["vartype"], dtype=np.uint8)
     keep.refs.append(vt)
     model.vartype = vt.ctypes.data_as(C.POINTER(C.c_ubyte))
     model.objshift = 0.0
