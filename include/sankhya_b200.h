@@ -223,8 +223,9 @@ SANKHYA_CUDA_API int sankhya_b200_pdlp_solve(
    reference's solve_qp (cuda/src/sankhya_cuda_lp.cu:36-52, 236-238; the CPU
    loop's c/src/sk_solve.c:908-923). The diagonal is taken exactly in the
    primal prox, x+ = proj((x - tau (c + A'y)) / (1 + tau q)); a general Q by a
-   gradient step, x+ = proj(x - tau (c + Q x + A'y)), its curvature along each
-   trial move entering the adaptive step's limit. Restarts, primal weight,
+   gradient step with a diagonal majorant, x+ = proj(x - tau (c + Q x + A'y) /
+   (1 + tau d)), d_j = sum_k |Q_jk| (Gershgorin, so the step is safe for Q at any
+   tau; for a diagonal Q the two forms coincide). Restarts, primal weight,
    precision modes and scaling (of A; Q is scaled by the column factors) are
    those of sankhya_b200_pdlp_solve, and the relative KKT uses the reduced cost
    c + Q x + A'y and the QP objectives (primal c'x + x'Qx/2, dual with -x'Qx/2).

@@ -135,10 +135,7 @@ __global__ void k_commit_dual(int n, int m, PdlpState* __restrict__ st, T* __res
 // programming using primal-dual hybrid gradient" (NeurIPS 2021, section 3.1).
 // For a trial move (dx, dy) made with step `used`, PDHG stays stable while the
 // step is at most  |dz|^2_w / (2 |dy' A dx|),  with |dz|^2_w = w |dx|^2 + |dy|^2 / w
-// (w the primal weight). With a quadratic objective taken by a gradient step (a
-// general Hessian Q) the smooth term's curvature along the move adds to the
-// coupling: the limit is |dz|^2_w / (2 |dy' A dx| + dx' Q dx), the local form of the
-// Condat-Vu condition 1/tau - sigma |A|^2 >= |Q| (cross = |dy' A dx| + dx' Q dx / 2). The move is kept when `used` is within that limit. The
+// (w the primal weight). The move is kept when `used` is within that limit. The
 // next step is min((1 - (k+1)^-0.3) limit, (1 + (k+1)^-0.6) used) for the k-th
 // trial: both factors tend to 1, so the step settles just under the limit.
 // With no interaction (or no movement) the limit is the largest allowed step;
@@ -169,7 +166,10 @@ enum QMode { kLp = 0, kQDiag = 1, kQGeneral = 2 };
 // K2 (PdlpKernels.cu:391-400 primal candidate + the |dx|^2 part of :405-430). QP:
 // diagonal q: x_cand = proj((x - tau (c + A'y)) / (1 + tau q)) (the prox of
 // c'x + q x^2 / 2 over the box, the reference's sankhya_cuda_lp.cu:36-52 form);
-// general Q: x_cand = proj(x - tau (c + Q x + A'y)), with Q x kept per column.
+// general Q: x_cand = proj(x - tau (c + Q x + A'y) / (1 + tau d)), the prox of the
+// linearised quadratic plus (x' - x)' D (x' - x) / 2 with the diagonal majorant
+// D = diag(d), d_j = sum_k |Q_jk| >= Q (Gershgorin), so the step is safe for Q at any
+// tau and only A's coupling limits it. With Q diagonal the two forms coincide.
 template <class T, int QM = kLp>
 struct PrimalCandEpi {
     const PdlpState* st;
@@ -177,21 +177,22 @@ struct PrimalCandEpi {
     const T* __restrict__ c;
     const T* __restrict__ cl;
     const T* __restrict__ cu;
-    const T* __restrict__ q;  // QM: the diagonal (kQDiag) or Q x (kQGeneral); unused for LP
+    const T* __restrict__ q;   // QM: the diagonal (kQDiag) or the majorant d (kQGeneral)
+    const T* __restrict__ qx;  // kQGeneral: Q x of the committed point
     T* __restrict__ x_cand;
     double* __restrict__ partial;
     using Acc = Slots<1, 1u>;
     struct Row {
-        T x, c, lo, hi, q;
+        T x, c, lo, hi, q, qx;
     };
     __device__ __forceinline__ Row load(int j) const {
-        return Row{x[j], c[j], cl[j], cu[j], QM == kLp ? T(0) : q[j]};
+        return Row{x[j], c[j], cl[j], cu[j], QM == kLp ? T(0) : q[j], QM == kQGeneral ? qx[j] : T(0)};
     }
     __device__ __forceinline__ void store(int j, T aty, const Row& r, Acc& acc) const {
         const T tau = static_cast<T>(st->eta / st->omega);
         T xc;
         if (QM == kQDiag) xc = clampf<T>((r.x - tau * (r.c + aty)) / (T(1) + tau * r.q), r.lo, r.hi);
-        else if (QM == kQGeneral) xc = clampf<T>(r.x - tau * (r.c + r.q + aty), r.lo, r.hi);
+        else if (QM == kQGeneral) xc = clampf<T>(r.x - tau * (r.c + r.qx + aty) / (T(1) + tau * r.q), r.lo, r.hi);
         else xc = clampf<T>(r.x - tau * (r.c + aty), r.lo, r.hi);
         x_cand[j] = xc;
         const double dx = static_cast<double>(xc) - static_cast<double>(r.x);
@@ -200,27 +201,19 @@ struct PrimalCandEpi {
     __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
 };
 
-// K3q (general Hessian): Q x_cand, and the curvature dx' Q dx = dx'(Q x_cand - Q x)
-// of the trial move in block partials, which K3's last block adds to the coupling.
-template <class T>
-struct QProbeEpi {
-    const T* __restrict__ x;
-    const T* __restrict__ x_cand;
-    const T* __restrict__ qx;
-    T* __restrict__ qx_cand;
-    double* __restrict__ partial;
-    using Acc = Slots<1, 1u>;
-    struct Row {
-        T x, xc, qx;
-    };
-    __device__ __forceinline__ Row load(int j) const { return Row{x[j], x_cand[j], qx[j]}; }
-    __device__ __forceinline__ void store(int j, T qxc, const Row& r, Acc& acc) const {
-        qx_cand[j] = qxc;
-        const double dx = static_cast<double>(r.xc) - static_cast<double>(r.x);
-        acc.add(0, dx * (static_cast<double>(qxc) - static_cast<double>(r.qx)));
+// Row sums of |Q| (the diagonal majorant of a symmetric Q), one warp per row.
+__global__ void k_abs_row_sums(int rows, const int* __restrict__ ptr, const double* __restrict__ val,
+                               double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int r = warp; r < rows; r += nwarps) {
+        double s = 0.0;
+        for (int p = ptr[r] + lane; p < ptr[r + 1]; p += 32) s += fabs(val[p]);
+        s = warp_sum(s);
+        if (lane == 0) out[r] = s;
     }
-    __device__ __forceinline__ void finish(Acc& acc, double* smem) const { block_store(acc, partial, smem); }
-};
+}
 
 // K3 (A x_cand, |dy|^2, dy.(A x_cand - A x), then PdlpKernels.cu:460-494 in the last block)
 template <class T>
@@ -233,8 +226,6 @@ struct ProbeEpi {
     double* __restrict__ partial;           // this kernel's [gridDim.x * 2]
     const double* __restrict__ partial_dx;  // K2's [grid_dx]
     int grid_dx;
-    const double* __restrict__ partial_q;   // K3q's [grid_q] curvature partials, or null
-    int grid_q;
     using Acc = Slots<2, 3u>;
     struct Row {
         T y, yc, ax;
@@ -258,34 +249,28 @@ struct ProbeEpi {
         if (!last) return;
         __threadfence();
         // fixed-order combine: thread k sums a strided slice, then a fixed tree
-        __shared__ double red[4][kThreads];
-        double a = 0.0, b = 0.0, d = 0.0, e = 0.0;
+        __shared__ double red[3][kThreads];
+        double a = 0.0, b = 0.0, d = 0.0;
         for (int g = threadIdx.x; g < grid_dx; g += kThreads) a += __ldcg(partial_dx + g);
         for (int g = threadIdx.x; g < static_cast<int>(gridDim.x); g += kThreads) {
             b += __ldcg(partial + 2 * g);
             d += __ldcg(partial + 2 * g + 1);
         }
-        if (partial_q)
-            for (int g = threadIdx.x; g < grid_q; g += kThreads) e += __ldcg(partial_q + g);
         red[0][threadIdx.x] = a;
         red[1][threadIdx.x] = b;
         red[2][threadIdx.x] = d;
-        red[3][threadIdx.x] = e;
         __syncthreads();
         for (int s = kThreads / 2; s > 0; s >>= 1) {
             if (threadIdx.x < s) {
                 red[0][threadIdx.x] += red[0][threadIdx.x + s];
                 red[1][threadIdx.x] += red[1][threadIdx.x + s];
                 red[2][threadIdx.x] += red[2][threadIdx.x + s];
-                red[3][threadIdx.x] += red[3][threadIdx.x + s];
             }
             __syncthreads();
         }
         if (threadIdx.x != 0) return;
         const double probe = st->updates + 1.0;
-        double cross = fabs(red[2][0]);
-        if (partial_q) cross += 0.5 * fmax(red[3][0], 0.0);
-        const StepRule rule = step_rule(st->eta, st->omega, red[0][0], red[1][0], cross, probe,
+        const StepRule rule = step_rule(st->eta, st->omega, red[0][0], red[1][0], fabs(red[2][0]), probe,
                                         st->eta_min, st->eta_max);
         st->dx_sq = red[0][0];
         st->dy_sq = red[1][0];
@@ -1181,15 +1166,15 @@ struct Core {
     int launches = 0;
     std::vector<cudaGraphExec_t> graphs;
     // Quadratic objective (the QP entry point): qmode kQDiag with the diagonal qd,
-    // or kQGeneral with the Hessian Q, whose products Q x (committed point),
-    // Q x_cand and Q x_avg ride along like the A-side ones; kLp otherwise.
+    // or kQGeneral with the Hessian Q and its diagonal majorant qd, whose products
+    // Q x (committed point), Q x_cand and Q x_avg ride along like the A-side ones;
+    // kLp otherwise.
     int qmode = kLp;
     const T* qd = nullptr;
     TileCsrT<T> Q;
     DevBuf qblob;
     T *qx = nullptr, *qx_cand = nullptr, *qx_avg = nullptr;
-    double* part_e = nullptr;
-    int grid_q = 1, grid_qs = 1;
+    int grid_qs = 1;
     // Centered mode (FP32 iterations of the FP32_REFINE precision): x, y, ax and the
     // sums are deviations from ctr's FP64 center; the center moves to the restart
     // point at every restart (one refinement), and the window-end residuals are
@@ -1258,26 +1243,23 @@ struct Core {
         graphs.clear();
     }
 
-    // The QP's Hessian: a diagonal (diag) or a general matrix (q, n x n); call after
-    // allocate and before set_problem. The general path owns Q x, Q x_cand, Q x_avg
-    // and the curvature partials.
+    // The QP's Hessian: a diagonal (diag, q null) or a general matrix (q, n x n, with
+    // diag its majorant row sums |Q|); call after allocate and before set_problem. The
+    // general path owns Q x, Q x_cand and Q x_avg.
     int set_hessian(const T* diag, const TileCsrT<T>* q) {
-        if (diag) {
+        if (!diag) return 0;
+        qd = diag;
+        if (!q) {
             qmode = kQDiag;
-            qd = diag;
             return 0;
         }
-        if (!q) return 0;
         qmode = kQGeneral;
         Q = *q;
         const size_t nb = (static_cast<size_t>(n) * sizeof(T) + 255) / 256 * 256;
-        const size_t pb = (static_cast<size_t>(sms) * 8 * 8 * 8 + 255) / 256 * 256;
-        if (qblob.alloc(3 * nb + pb, "cudaMalloc Hessian products")) return -1;
+        if (qblob.alloc(3 * nb, "cudaMalloc Hessian products")) return -1;
         qx = qblob.as<T>();
         qx_cand = reinterpret_cast<T*>(qblob.as<char>() + nb);
         qx_avg = reinterpret_cast<T*>(qblob.as<char>() + 2 * nb);
-        part_e = reinterpret_cast<double*>(qblob.as<char>() + 3 * nb);
-        grid_q = tiled_grid<QProbeEpi<T>, T>(Q);
         grid_qs = tiled_grid<StoreEpiT<T>, T>(Q);
         return 0;
     }
@@ -1328,18 +1310,19 @@ struct Core {
         ++launches;
         if (!make_candidate) return;
         if (qmode == kQDiag)
-            launch_tiled(AT, y_cand, PrimalCandEpi<T, kQDiag>{st, x, c, cl, cu, qd, x_cand, part_c}, stream, grid_k2);
+            launch_tiled(AT, y_cand, PrimalCandEpi<T, kQDiag>{st, x, c, cl, cu, qd, nullptr, x_cand, part_c}, stream,
+                         grid_k2);
         else if (general)
-            launch_tiled(AT, y_cand, PrimalCandEpi<T, kQGeneral>{st, x, c, cl, cu, qx, x_cand, part_c}, stream,
+            launch_tiled(AT, y_cand, PrimalCandEpi<T, kQGeneral>{st, x, c, cl, cu, qd, qx, x_cand, part_c}, stream,
                          grid_k2);
         else
-            launch_tiled(AT, y_cand, PrimalCandEpi<T>{st, x, c, cl, cu, nullptr, x_cand, part_c}, stream, grid_k2);
+            launch_tiled(AT, y_cand, PrimalCandEpi<T>{st, x, c, cl, cu, nullptr, nullptr, x_cand, part_c}, stream,
+                         grid_k2);
         if (general) {
-            launch_tiled(Q, x_cand, QProbeEpi<T>{x, x_cand, qx, qx_cand, part_e}, stream, grid_q);
+            launch_tiled(Q, x_cand, StoreEpiT<T>{qx_cand}, stream, grid_qs);   // Q x_cand, committed with x_cand
             ++launches;
         }
-        launch_tiled(A, x_cand, ProbeEpi<T>{st, y, y_cand, ax, ax_cand, part_d, part_c, AT.ntiles ? grid_k2 : 0,
-                                            general ? part_e : nullptr, Q.ntiles ? grid_q : 0},
+        launch_tiled(A, x_cand, ProbeEpi<T>{st, y, y_cand, ax, ax_cand, part_d, part_c, AT.ntiles ? grid_k2 : 0},
                      stream, grid_k3);
         launches += 2;
     }
@@ -1804,19 +1787,24 @@ int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, cons
     int refinements = 0;
     int launches = sc.launches;
 
-    // QP: the Hessian in the scaled space, Q' = C Q C (a diagonal q' = C^2 q)
+    // QP: the Hessian in the scaled space, Q' = C Q C (a diagonal q' = C^2 q); for a
+    // general Q also its diagonal majorant d_j = sum_k |Q'_jk|
     std::shared_ptr<Plan> qplan;
     DevBuf qbuf;
     TileCsr Qs;
     double* qd_s = nullptr;
     if (hessian) {
         if (get_plan(hessian, &qplan)) return -1;
-        if (qbuf.alloc(static_cast<size_t>(qplan->a.nnz) * 8 + 256, "cudaMalloc scaled Hessian")) return -1;
+        const size_t qv = (static_cast<size_t>(qplan->a.nnz) * 8 + 255) / 256 * 256;
+        if (qbuf.alloc(qv + static_cast<size_t>(n) * 8 + 256, "cudaMalloc scaled Hessian")) return -1;
         Qs = qplan->a;
         Qs.val = qbuf.as<double>();
-        k_scale_values<<<std::min((n + 7) / 8 + 1, sc.sms * 16), kThreads, 0, stream>>>(
-            n, qplan->a.ptr, qplan->a.idx, qplan->a.val, sc.Cs, sc.Cs, 0, qbuf.as<double>());
-        ++launches;
+        qd_s = reinterpret_cast<double*>(qbuf.as<char>() + qv);
+        const int wg = std::min((n + 7) / 8 + 1, sc.sms * 16);
+        k_scale_values<<<wg, kThreads, 0, stream>>>(n, qplan->a.ptr, qplan->a.idx, qplan->a.val, sc.Cs, sc.Cs, 0,
+                                                    qbuf.as<double>());
+        k_abs_row_sums<<<wg, kThreads, 0, stream>>>(n, qplan->a.ptr, Qs.val, qd_s);
+        launches += 2;
     } else if (qdiag) {
         if (qbuf.alloc(static_cast<size_t>(n) * 8 + 256, "cudaMalloc scaled Hessian diagonal")) return -1;
         qd_s = qbuf.as<double>();
@@ -1885,12 +1873,16 @@ int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, cons
         ctr.qdiag = qd_s;
         if (hessian) {
             ctr.Q = Qs;
+            ctr.qdiag = nullptr;   // the centered residuals take Q x_center, not a diagonal
             ctr.qx_c = reinterpret_cast<double*>(cbuf.as<char>() + 2 * nd + md);
             ctr.grid_q = tiled_grid<StoreEpi>(Qs);
             const size_t qnnz = static_cast<size_t>(Qs.nnz);
-            if (q32buf.alloc(qnnz * 4 + 256, "cudaMalloc FP32 Hessian")) return -1;
+            const size_t qv32 = (qnnz * 4 + 255) / 256 * 256;
+            if (q32buf.alloc(qv32 + static_cast<size_t>(n) * 4 + 256, "cudaMalloc FP32 Hessian")) return -1;
             k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(qnnz), Qs.val, q32buf.as<float>());
             Q32 = Qs.with_values<float>(q32buf.as<float>());
+            qd32 = reinterpret_cast<float*>(q32buf.as<char>() + qv32);
+            k_narrow<<<eg(n), kThreads, 0, stream>>>(n, qd_s, qd32);
         } else if (qdiag) {
             if (q32buf.alloc(static_cast<size_t>(n) * 4 + 256, "cudaMalloc FP32 Hessian diagonal")) return -1;
             qd32 = q32buf.as<float>();
