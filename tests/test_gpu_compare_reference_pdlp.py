@@ -1,12 +1,9 @@
 """The engine's PDLP against the reference C++ core's own GPU PDLP (GpuPdlp, with the
 scaling of run_first_order, src/lp/LpSolver.cpp:62-99), both on the same B200, on
 seeded instances: both must converge to 1e-6 relative KKT and agree on the objective;
-iterations and seconds are printed side by side.
-
-Run on demand with `python -m pytest tests/compare_reference_pdlp.py -s`: the file name
-keeps it out of the default collection until it has run on a B200 (it needs
+iterations and seconds are printed side by side (`-s`). It needs
 oracle/_ref/libsihps_pdlp_ref.so, built by `make -C oracle ref` where the reference
-sources are)."""
+sources are, and skips without it."""
 import os
 
 import numpy as np
