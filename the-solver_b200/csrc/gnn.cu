@@ -11,14 +11,18 @@
 //   y_hat = ys (Hc wy + by)
 //   loss  = mean ((x_hat - x*) / width)^2 + mean ((y_hat - y*) / ys)^2
 //
-// Dense layers run on the tensor cores: mma.sync m16n8k16 with bf16 operands and
-// fp32 accumulation (inputs rounded to bf16 when staged in shared memory). Their
-// K is 16 or 128 and N is 64, so they are HBM-bound streams of the activations,
-// not tensor-throughput-bound. Aggregations are fp32 gathers over the stored A
+// Dense layers run on the tensor cores with bf16 operands and fp32 accumulation
+// (inputs rounded to bf16 when staged in shared memory): the layer products and
+// the input gradients (K = 16, 64 or 128; N = 64 or 128) on the 5th-generation
+// tensor cores, tcgen05.mma with a TMEM accumulator (tc_gemm.cuh); the weight
+// gradients, which reduce over all nodes, by an mma.sync m16n8k16 kernel split
+// over node slices. They are HBM-bound streams of the activations, not
+// tensor-throughput-bound. Aggregations are fp32 gathers over the stored A
 // and A' (warp per node, 64 channels, entries in stored order). Every reduction
 // (weight gradients split over K, bias sums, head sums, loss) has a fixed order,
 // so a training run is reproducible bit for bit.
 #include "batch_common.cuh"
+#include "tc_gemm.cuh"
 
 #include <cuda_bf16.h>
 
@@ -515,6 +519,8 @@ struct SankhyaB200Gnn {
     std::vector<float*> xv, xc;       // rounds + 1 layer inputs [n|m x 128]
     float *gv = nullptr, *gc = nullptr, *zv = nullptr, *zc = nullptr, *part = nullptr, *lossf = nullptr;
     FeatureSlots* slots = nullptr;
+    DevBuf tc_flag;                   // set by a tensor-core GEMM whose bounded wait gave up
+    int sms = 148;
 };
 
 namespace b200 {
@@ -574,19 +580,59 @@ int ensure_workspace(SankhyaB200Gnn* g, int m, int n) {
     return 0;
 }
 
+// The tensor-core (tcgen05) GEMM where its layout conditions hold: 16-byte
+// aligned rows of A and C (row strides multiples of 4 floats). One CTA per SM-share
+// of TMEM (512 columns per SM, N per CTA), persistent over the 128-row tiles.
+bool tc_fits(const void* a, int lda, const void* c, int ldc) {
+    return (reinterpret_cast<uintptr_t>(a) & 15u) == 0 && (reinterpret_cast<uintptr_t>(c) & 15u) == 0 &&
+           lda % 4 == 0 && ldc % 4 == 0;
+}
+
+template <int N, int K>
+void gemm_tc(SankhyaB200Gnn* s, cudaStream_t st, int M, const float* A, int lda, const __nv_bfloat16* B, int sbk,
+             int sbn, const float* bias, int relu, float* C, int ldc) {
+    using S = tc::TcShape<N, K>;
+    const void* fn = reinterpret_cast<const void*>(&tc::k_gemm_tc<N, K>);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmem);
+    const int tiles = (M + S::kM - 1) / S::kM;
+    const int grid = std::max(1, std::min(tiles, s->sms * std::min(4, 512 / S::kCols)));
+    tc::k_gemm_tc<N, K><<<grid, 128, S::kSmem, st>>>(M, A, lda, B, sbk, sbn, bias, relu, C, ldc,
+                                                     s->tc_flag.as<unsigned int>());
+}
+
 // C = A B (+ bias, relu) with A fp32 [M x K] (row-major, lda) and B bf16 [K x 64] row-major.
-void gemm_forward(cudaStream_t st, int M, int K, const float* A, int lda, const __nv_bfloat16* W, const float* bias,
-                  float* C, int ldc) {
+void gemm_forward(SankhyaB200Gnn* s, cudaStream_t st, int M, int K, const float* A, int lda,
+                  const __nv_bfloat16* W, const float* bias, float* C, int ldc) {
     if (M == 0) return;
+    if (tc_fits(A, lda, C, ldc) && (K == kF || K == kX)) {
+        if (K == kF) gemm_tc<kH, kF>(s, st, M, A, lda, W, kH, 1, bias, 1, C, ldc);
+        else gemm_tc<kH, kX>(s, st, M, A, lda, W, kH, 1, bias, 1, C, ldc);
+        return;
+    }
     Gemm<__nv_bfloat16> g{M, kH, K, A, lda, 1, W, kH, 1, C, ldc, 1, 0, K, bias, 1};
     k_gemm_bf16<__nv_bfloat16><<<dim3((M + 63) / 64, 1, 1), kGemmThreads, 0, st>>>(g);
 }
 
 // dX [M x K] = dZ [M x 64] W^T, W bf16 [K x 64] row-major; K = 128.
-void gemm_input_grad(cudaStream_t st, int M, const float* dz, const __nv_bfloat16* W, int K, float* dx, int ldx) {
+void gemm_input_grad(SankhyaB200Gnn* s, cudaStream_t st, int M, const float* dz, const __nv_bfloat16* W, int K,
+                     float* dx, int ldx) {
     if (M == 0) return;
+    if (tc_fits(dz, kH, dx, ldx) && K == kX) {
+        gemm_tc<kX, kH>(s, st, M, dz, kH, W, 1, kH, nullptr, 0, dx, ldx);
+        return;
+    }
     Gemm<__nv_bfloat16> g{M, K, kH, dz, kH, 1, W, 1, kH, dx, ldx, 1, 0, kH, nullptr, 0};
     k_gemm_bf16<__nv_bfloat16><<<dim3((M + 63) / 64, (K + 63) / 64, 1), kGemmThreads, 0, st>>>(g);
+}
+
+// Fails the call when a tensor-core GEMM's bounded wait gave up (the flag is cleared).
+int check_tc(SankhyaB200Gnn* s, cudaStream_t st) {
+    unsigned int flag = 0;
+    B200_TRY(cudaMemcpyAsync(&flag, s->tc_flag.p, sizeof(flag), cudaMemcpyDeviceToHost, st), "read GEMM flag");
+    B200_TRY(cudaStreamSynchronize(st), "network");
+    if (!flag) return 0;
+    cudaMemsetAsync(s->tc_flag.p, 0, sizeof(flag), st);
+    return fail_msg("a tensor-core GEMM's wait for its MMAs gave up");
 }
 
 // dW [K x 64] = X^T dZ over `rows` nodes (X fp32 [rows x K] with row stride ldx),
@@ -643,13 +689,13 @@ int upload_instance(SankhyaB200Gnn* g, const Plan& plan, const double* c, const 
 void forward(SankhyaB200Gnn* g, const Plan& plan, cudaStream_t st) {
     const int m = plan.a.rows, n = plan.a.cols, R = g->settings.rounds;
     const Offsets& o = g->off;
-    gemm_forward(st, n, kF, g->fv, kF, g->params_h + o.Ev, g->params + o.bev, g->xv[0], kX);
-    gemm_forward(st, m, kF, g->fc, kF, g->params_h + o.Ec, g->params + o.bec, g->xc[0], kX);
+    gemm_forward(g, st, n, kF, g->fv, kF, g->params_h + o.Ev, g->params + o.bev, g->xv[0], kX);
+    gemm_forward(g, st, m, kF, g->fc, kF, g->params_h + o.Ec, g->params + o.bec, g->xc[0], kX);
     for (int t = 0; t < R; ++t) {
         spmm(st, plan.a, g->xv[t], kX, nullptr, g->inv_row, g->xc[t] + kH, kX, 0);
-        gemm_forward(st, m, kX, g->xc[t], kX, g->params_h + o.Wc[t], g->params + o.bc[t], g->xc[t + 1], kX);
+        gemm_forward(g, st, m, kX, g->xc[t], kX, g->params_h + o.Wc[t], g->params + o.bc[t], g->xc[t + 1], kX);
         spmm(st, plan.at, g->xc[t + 1], kX, nullptr, g->inv_col, g->xv[t] + kH, kX, 0);
-        gemm_forward(st, n, kX, g->xv[t], kX, g->params_h + o.Wv[t], g->params + o.bv[t], g->xv[t + 1], kX);
+        gemm_forward(g, st, n, kX, g->xv[t], kX, g->params_h + o.Wv[t], g->params + o.bv[t], g->xv[t + 1], kX);
     }
 }
 
@@ -687,7 +733,7 @@ void backward(SankhyaB200Gnn* g, const Plan& plan, cudaStream_t st) {
                                                                                      g->zv);
         gemm_weight_grad(g, st, n, g->xv[t], kX, kX, g->zv, g->grad + o.Wv[t]);
         bias_grad(g, st, n, g->zv, g->grad + o.bv[t]);
-        gemm_input_grad(st, n, g->zv, g->params_h + o.Wv[t], kX, g->gv, kX);
+        gemm_input_grad(g, st, n, g->zv, g->params_h + o.Wv[t], kX, g->gv, kX);
         spmm(st, plan.a, g->gv + kH, kX, g->inv_col, nullptr, g->gc, kX, 1);
         if (m) {
             k_relu_mask<<<elem_blocks(static_cast<long long>(m) * kH), kThreads, 0, st>>>(m, g->gc, kX, g->xc[t + 1],
@@ -696,7 +742,7 @@ void backward(SankhyaB200Gnn* g, const Plan& plan, cudaStream_t st) {
         gemm_weight_grad(g, st, m, g->xc[t], kX, kX, g->zc, g->grad + o.Wc[t]);
         if (m) {
             bias_grad(g, st, m, g->zc, g->grad + o.bc[t]);
-            gemm_input_grad(st, m, g->zc, g->params_h + o.Wc[t], kX, g->gc, kX);
+            gemm_input_grad(g, st, m, g->zc, g->params_h + o.Wc[t], kX, g->gc, kX);
         } else {
             cudaMemsetAsync(g->grad + o.bc[t], 0, sizeof(float) * kH, st);
         }
@@ -755,7 +801,7 @@ int upload_targets(SankhyaB200Gnn* g, int m, int n, const double* x_t, const dou
 int read_loss(SankhyaB200Gnn* g, cudaStream_t st, double* loss) {
     float l[2] = {0.f, 0.f};
     B200_TRY(cudaMemcpyAsync(l, g->lossf, sizeof(l), cudaMemcpyDeviceToHost, st), "read loss");
-    B200_TRY(cudaStreamSynchronize(st), "network step");
+    if (check_tc(g, st)) return -1;
     if (loss) *loss = static_cast<double>(l[0]) + static_cast<double>(l[1]);
     return 0;
 }
@@ -795,10 +841,13 @@ extern "C" int sankhya_b200_gnn_create(const SankhyaB200GnnSettings* settings, S
     g->off = param_offsets(s.rounds);
     const long long P = g->off.total;
     const long long fb = (4 * P + 255) / 256 * 256, hb = (2 * P + 255) / 256 * 256;
-    if (g->model.alloc(static_cast<size_t>(4 * fb + hb), "cudaMalloc network parameters")) {
+    if (g->model.alloc(static_cast<size_t>(4 * fb + hb), "cudaMalloc network parameters") ||
+        g->tc_flag.alloc(256, "cudaMalloc GEMM flag") ||
+        cudaMemset(g->tc_flag.p, 0, 256) != cudaSuccess) {
         delete g;
         return -1;
     }
+    cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, g->device);
     char* p = g->model.as<char>();
     g->params = reinterpret_cast<float*>(p);
     g->grad = reinterpret_cast<float*>(p + fb);
@@ -880,8 +929,7 @@ extern "C" int sankhya_b200_gnn_predict(SankhyaB200Gnn* g, const SankhyaCudaCSR*
     B200_TRY(cudaGetLastError(), "network forward");
     B200_TRY(cudaMemcpyAsync(x_out, g->x_hat, 8LL * n, cudaMemcpyDeviceToHost, st), "read prediction");
     if (y_out && m) B200_TRY(cudaMemcpyAsync(y_out, g->y_hat, 8LL * m, cudaMemcpyDeviceToHost, st), "read prediction");
-    B200_TRY(cudaStreamSynchronize(st), "network forward");
-    return 0;
+    return check_tc(g, st);
 }
 
 extern "C" int sankhya_b200_gnn_gradient(SankhyaB200Gnn* g, const SankhyaCudaCSR* matrix, const double* c,
