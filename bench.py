@@ -324,20 +324,23 @@ def _pdlp_run(E, A, inst, eps, precision, algorithm, limit_s, oracle):
     return out
 
 
-def time_to_kkt(E, A, inst, eps_list=(1e-4, 1e-6, 1e-8), limit_s=120.0, halpern=False):
+def time_to_kkt(E, A, inst, eps_list=(1e-4, 1e-6, 1e-8), limit_s=120.0, halpern=False, limit_1e8_s=60.0):
     """Wall time of sankhya_b200_pdlp_solve to each relative-KKT tolerance on the same
     instance: plain FP64 PDLP (GpuPdlp's restarted adaptive loop) versus FP32 inner
     iterations refined in FP64 at every restart. Host arrays in and out, scaling
     included. Each run's objective is compared with the FP64 oracle value of the
-    instance (solved to 1e-9 by two independent FP64 solvers) where it is present.
-    With halpern, the reflected restarted Halpern loop runs at the middle tolerance."""
+    instance (the tightest FP64 solves of two independent codes) where it is present.
+    With halpern, the reflected restarted Halpern loop runs at the middle tolerance.
+    Tolerances below 1e-7 get limit_1e8_s: the restarted loop stalls near a 2e-6 gap on
+    the bench instance, so those runs report where they stopped."""
     oracle = oracle_objective()
     out = {"relative_kkt": "max(primal, dual, gap) as in GpuPdlp", "oracle_objective": oracle,
-           "oracle": "tests/golden/objective_lp_config1.json (FP64 PDLP to 1e-9: engine, and the reference's GpuPdlp)"}
+           "oracle": "tests/golden/objective_lp_config1.json (the reference's GpuPdlp and the engine, FP64, tightest)"}
     for eps in eps_list:
         key = f"eps_{eps:.0e}"
-        row = {"fp64": _pdlp_run(E, A, inst, eps, E.FP64, E.PDLP_ADAPTIVE, limit_s, oracle),
-               "fp32_refined": _pdlp_run(E, A, inst, eps, E.FP32_REFINE, E.PDLP_ADAPTIVE, limit_s, oracle)}
+        lim = limit_1e8_s if eps < 1e-7 else limit_s
+        row = {"fp64": _pdlp_run(E, A, inst, eps, E.FP64, E.PDLP_ADAPTIVE, lim, oracle),
+               "fp32_refined": _pdlp_run(E, A, inst, eps, E.FP32_REFINE, E.PDLP_ADAPTIVE, lim, oracle)}
         if halpern and eps == eps_list[len(eps_list) // 2]:
             row["halpern_fp64"] = _pdlp_run(E, A, inst, eps, E.FP64, E.PDLP_HALPERN, limit_s, oracle)
         for name in [k for k in row if k != "fp64"]:
