@@ -616,6 +616,7 @@ def run_qp(args):
         for label, prec in (("fp64", E.FP64), ("fp32_refined", E.FP32_REFINE)):
             ps_ = E.pdlp_default_settings()
             ps_.eps_optimal, ps_.precision, ps_.time_limit, ps_.max_iterations = 1e-6, prec, 120.0, 20_000_000
+            E.pdlp_solve_qp(A, inst, ps_, **kw)       # warm-up: plans, graphs, attributes
             t0 = time.perf_counter()
             rc, x, y, r = E.pdlp_solve_qp(A, inst, ps_, **kw)
             wall = time.perf_counter() - t0

@@ -142,7 +142,9 @@ def test_config0_to_1e8_reaches_the_simplex_objective(engine, instances, golden_
 def test_fp32_refined_agrees_with_fp64_on_power_law(engine, instances):
     """|a| over six decades. The restarted loop's progress past ~1e-5 on such matrices
     depends on the exact rounding of its trajectory (FP64 runs of two implementations
-    stall at different gaps), so the check is at 1e-5, where both converge."""
+    stall at different gaps), so the check is at 1e-5, where both converge. A relative
+    gap of 1e-5 (over 1 + |primal| + |dual|) leaves each objective up to ~2e-5 from
+    the optimum, so two converged points agree to 1e-4."""
     inst = instances.lp_powerlaw(21, 4000, 8000, 80000)
     A = engine.Matrix.from_instance(inst)
     rc64, x64, y64, r64 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-5, time_limit=60.0))
@@ -150,7 +152,7 @@ def test_fp32_refined_agrees_with_fp64_on_power_law(engine, instances):
                                                               time_limit=60.0))
     assert rc64 == 0 and rc32 == 0 and r64["status"] == 0 and r32["status"] == 0, (r64, r32)
     o64, o32 = float(np.dot(inst["c"], x64)), float(np.dot(inst["c"], x32))
-    assert abs(o64 - o32) <= 1e-5 * (1 + abs(o64))
+    assert abs(o64 - o32) <= 1e-4 * (1 + abs(o64))
 
 
 @pytest.mark.parametrize("eps", [1e-6, 1e-8])
