@@ -5,8 +5,11 @@ shared-memory descriptor of the canonical K-major layout without swizzle (versio
 leading byte offset = the K-adjacent core matrix, stride byte offset = the next 8-row
 block), the kind::f16 instruction descriptor for bf16 x bf16 -> fp32 at M = 128,
 N = 64 and 128, and the element offsets of the staged tiles against CuTe's stated
-canonical form ((8, m), (8, 2)) : ((8, SBO), (1, LBO)). Uses the CUTLASS headers
-vendored with flashinfer; skips where they or nvcc are absent."""
+canonical form ((8, m), (8, 2)) : ((8, SBO), (1, LBO)); and for the weight-gradient
+kernel's MN-major operands, the descriptor that CuTe's own make_umma_desc<Major::MN>
+derives from the layout ((8, MN/8), (8, 2)) : ((1, 64), (8, LBO/2)) (elements), the
+element offsets of that layout, and the instruction descriptor with both major bits.
+Uses the CUTLASS headers vendored with flashinfer; skips where they or nvcc are absent."""
 import importlib.util
 import os
 import shutil
@@ -18,10 +21,34 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 
 SOURCE = r"""
 #include <cstdio>
-#include <cute/arch/mma_sm100_desc.hpp>
+#include <cute/tensor.hpp>
+#include <cute/atom/mma_traits_sm100.hpp>
 #include "tc_gemm.cuh"
-int main() {
+template <int MN, int LBOE>
+int check_mn() {
+    using namespace cute;
     int bad = 0;
+    auto L = make_layout(make_shape(make_shape(_8{}, Int<MN / 8>{}), make_shape(_8{}, _2{})),
+                         make_stride(make_stride(_1{}, _64{}), make_stride(_8{}, Int<LBOE>{})));
+    auto t = make_tensor(make_smem_ptr(reinterpret_cast<cutlass::bfloat16_t*>(0)), L);
+    UMMA::SmemDescriptor d = UMMA::make_umma_desc<UMMA::Major::MN>(t);
+    d.start_address_ = 0;
+    if (uint64_t(d) != b200::tc::smem_desc(0, LBOE * 2, 128)) ++bad;
+    for (int mn = 0; mn < MN; ++mn) for (int k = 0; k < 16; ++k)
+        if (unsigned(L(mn, k)) * 2 != b200::tc::mnmajor_offset<MN>(mn, k)) ++bad;
+    return bad;
+}
+int main() {
+    int bad = check_mn<128, 1024>() + check_mn<64, 512>();
+    {
+        cute::UMMA::InstrDescriptor i;
+        i.desc_ = 0;
+        i.c_format_ = 1;
+        i.a_format_ = uint8_t(cute::UMMA::F16F32Format::BF16);
+        i.b_format_ = uint8_t(cute::UMMA::F16F32Format::BF16);
+        i.a_major_ = 1; i.b_major_ = 1; i.n_dim_ = 64 >> 3; i.m_dim_ = 128 >> 4;
+        if (uint32_t(i) != b200::tc::instr_desc_bf16_mn(128, 64)) ++bad;
+    }
     const unsigned addrs[] = {0u, 1024u, 49152u, 65792u};
     const unsigned Ks[] = {16u, 64u, 128u};
     for (unsigned a : addrs) for (unsigned K : Ks) {

@@ -14,10 +14,11 @@
 // Dense layers run on the tensor cores with bf16 operands and fp32 accumulation
 // (inputs rounded to bf16 when staged in shared memory): the layer products and
 // the input gradients (K = 16, 64 or 128; N = 64 or 128) on the 5th-generation
-// tensor cores, tcgen05.mma with a TMEM accumulator (tc_gemm.cuh); the weight
-// gradients, which reduce over all nodes, by an mma.sync m16n8k16 kernel split
-// over node slices. They are HBM-bound streams of the activations, not
-// tensor-throughput-bound. Aggregations are fp32 gathers over the stored A
+// tensor cores, tcgen05.mma with a TMEM accumulator (tc_gemm.cuh), and so are
+// the weight gradients of the 128-wide layers, which reduce over all nodes in
+// fixed node slices; the 16-wide input layers' weight gradients and any operand
+// that is not 16-byte aligned take an mma.sync m16n8k16 kernel. They are
+// HBM-bound streams of the activations, not tensor-throughput-bound. Aggregations are fp32 gathers over the stored A
 // and A' (warp per node, 64 channels, entries in stored order). Every reduction
 // (weight gradients split over K, bias sums, head sums, loss) has a fixed order,
 // so a training run is reproducible bit for bit.
@@ -156,29 +157,36 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(Gemm<TB> g) {
 }
 
 // out[i] = sum over z of part[z stride + i]. A block covers 64 consecutive
-// outputs with four slice phases (z = q mod 4); each thread keeps eight
-// accumulators (z = q + 4 u mod 32), summed by a fixed tree, and the phases are
-// combined in order: a fixed order for every output, with short load chains.
-__global__ void __launch_bounds__(4 * kH) k_sum_slices(int count, int slices, long long stride,
-                                                       const float* __restrict__ part, float* __restrict__ out) {
-    __shared__ float red[4][kH];
-    const int c = blockIdx.x * kH + (threadIdx.x & (kH - 1)), q = threadIdx.x >> 6;
+// outputs with sixteen slice phases (z = q mod 16); each thread keeps eight
+// accumulators (z = q + 16 u mod 128), summed by a fixed tree, and the phases are
+// combined by a fixed tree: a fixed order for every output, and eight independent
+// loads in flight per thread.
+constexpr int kSumPhases = 16;
+
+__global__ void __launch_bounds__(kSumPhases * kH) k_sum_slices(int count, int slices, long long stride,
+                                                                const float* __restrict__ part,
+                                                                float* __restrict__ out) {
+    __shared__ float red[kSumPhases][kH];
+    const int i = threadIdx.x & (kH - 1), q = threadIdx.x >> 6;
+    const int c = blockIdx.x * kH + i;
     float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (c < count)
-        for (int z0 = q; z0 < slices; z0 += 32)
+        for (int z0 = q; z0 < slices; z0 += 8 * kSumPhases)
 #pragma unroll
             for (int u = 0; u < 8; ++u)
-                if (z0 + 4 * u < slices) a[u] += part[(z0 + 4 * u) * stride + c];
-    red[q][threadIdx.x & (kH - 1)] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+                if (z0 + kSumPhases * u < slices) a[u] += part[(z0 + kSumPhases * u) * stride + c];
+    red[q][i] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
     __syncthreads();
     if (q == 0 && c < count) {
-        const int i = threadIdx.x;
-        out[c] = (red[0][i] + red[1][i]) + (red[2][i] + red[3][i]);
+        float r[8];
+#pragma unroll
+        for (int h = 0; h < 8; ++h) r[h] = red[2 * h][i] + red[2 * h + 1][i];
+        out[c] = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
     }
 }
 
 void sum_slices(int count, int slices, long long stride, const float* part, float* out, cudaStream_t st) {
-    k_sum_slices<<<(count + kH - 1) / kH, 4 * kH, 0, st>>>(count, slices, stride, part, out);
+    k_sum_slices<<<(count + kH - 1) / kH, kSumPhases * kH, 0, st>>>(count, slices, stride, part, out);
 }
 
 // --------------------------------------------------------- aggregation
@@ -617,7 +625,7 @@ void gemm_forward(SankhyaB200Gnn* s, cudaStream_t st, int M, int K, const float*
 void gemm_input_grad(SankhyaB200Gnn* s, cudaStream_t st, int M, const float* dz, const __nv_bfloat16* W, int K,
                      float* dx, int ldx) {
     if (M == 0) return;
-    if (tc_fits(dz, kH, dx, ldx) && K == kX) {
+    if (tc_fits(dz, kH, dx, ldx) && K == kX && (reinterpret_cast<uintptr_t>(W) & 15u) == 0) {
         gemm_tc<kX, kH>(s, st, M, dz, kH, W, 1, kH, nullptr, 0, dx, ldx);
         return;
     }
@@ -641,6 +649,19 @@ void gemm_weight_grad(SankhyaB200Gnn* s, cudaStream_t st, int rows, const float*
                       float* out) {
     if (rows == 0) {
         cudaMemsetAsync(out, 0, sizeof(float) * K * kH, st);
+        return;
+    }
+    if (K == kX && tc_fits(X, ldx, dz, kH)) {
+        // tensor-core path: slices of a whole number of 64-node stages, at most 2 per SM
+        const int stage = tc::WgShape::kNodes;
+        const int want = std::max(1, std::min(148 * 2, (rows + 255) / 256));
+        const int chunk = ((rows + want - 1) / want + stage - 1) / stage * stage;
+        const int slices = (rows + chunk - 1) / chunk;
+        const void* fn = reinterpret_cast<const void*>(&tc::k_wgrad_tc<kX>);
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::WgShape::kSmem);
+        tc::k_wgrad_tc<kX><<<slices, 128, tc::WgShape::kSmem, st>>>(rows, chunk, X, ldx, dz, s->part,
+                                                                 s->tc_flag.as<unsigned int>());
+        sum_slices(K * kH, slices, static_cast<long long>(K) * kH, s->part, out, st);
         return;
     }
     const int slices = std::max(1, std::min(148 * 2, (rows + 255) / 256));

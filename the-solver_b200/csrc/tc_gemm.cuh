@@ -11,12 +11,19 @@
 // threads round A to bf16 into shared memory in the canonical K-major layout
 // without swizzle (8 x 16-byte core matrices; core (row block i, k block j) at
 // (i K/8 + j) 128 bytes, so the K-adjacent core is 128 bytes away (leading byte
-// offset) and the next 8-row block K/8 * 128 bytes (stride byte offset)); thread
-// 0 issues K/16 MMAs of 128 x N x 16 and commits them to an mbarrier; after the
-// wait each warp reads its 32 rows (TMEM lanes 32w..32w+31) with tcgen05.ld and
-// applies bias / relu. The operands are rounded to bf16 exactly as the mma.sync
-// kernel rounds them; only the fp32 accumulation order inside the tensor core
-// differs.
+// offset) and the next 8-row block K/8 * 128 bytes (stride byte offset)). The
+// staging is by 32-byte pieces (8 k of one row) numbered so that piece u lands at
+// byte 16 u: each thread keeps up to 8 pieces (16 float4 loads) in flight, and the
+// first pieces of its next tile are loaded while the current tile's MMAs and
+// epilogue run. Thread 0 issues K/16 MMAs of 128 x N x 16 and commits them to an
+// mbarrier; after the wait each warp reads its 32 rows (TMEM lanes 32w..32w+31)
+// with tcgen05.ld, applies bias / relu and transposes 32 x 16 blocks through shared
+// memory so that its stores cover 64 contiguous bytes of 8 rows at a time. The
+// operands are rounded to bf16 exactly as the mma.sync kernel rounds them; only
+// the fp32 accumulation order inside the tensor core differs.
+//
+// k_wgrad_tc (below) computes the weight gradients X^T dZ with both operands
+// MN-major, summed over node slices in a fixed order.
 //
 // Descriptor bitfields follow CUTLASS's cute/arch/mma_sm100_desc.hpp
 // (SmemDescriptor, InstrDescriptor); tests/test_tc_descriptors.py checks them on
@@ -42,6 +49,21 @@ __host__ __device__ constexpr uint64_t smem_desc(uint32_t saddr, uint32_t lbo_by
 __host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
            (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+// The same with A and B both MN-major (bits 15 and 16): A's M and B's N index is the
+// contiguous one inside a 16-byte core row.
+__host__ __device__ constexpr uint32_t instr_desc_bf16_mn(int M, int N) {
+    return instr_desc_bf16(M, N) | (1u << 15) | (1u << 16);
+}
+
+// Byte offset of element (mn, k) in the canonical MN-major layout without swizzle used
+// by the weight-gradient kernel: a core matrix is 8 k-rows of 16 bytes (8 consecutive
+// mn), the next 8 mn are 128 bytes away (stride byte offset) and the next 8 k are
+// (MN / 8) * 128 bytes away (leading byte offset).
+template <int MN>
+__host__ __device__ constexpr uint32_t mnmajor_offset(int mn, int k) {
+    return static_cast<uint32_t>((k >> 3) * (MN / 8) * 128 + (mn >> 3) * 128 + (k & 7) * 16 + (mn & 7) * 2);
 }
 
 // Byte offset of element (r, k) in the canonical K-major tile with K columns.
@@ -70,6 +92,44 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, long lon
 
 constexpr long long kWaitLimit = 1ll << 22;
 
+// 8 fp32 -> 8 bf16 (16 bytes), round to nearest even.
+__device__ __forceinline__ uint4 pack8(const float4& a, const float4& b) {
+    __nv_bfloat162 p0 = __floats2bfloat162_rn(a.x, a.y), p1 = __floats2bfloat162_rn(a.z, a.w);
+    __nv_bfloat162 p2 = __floats2bfloat162_rn(b.x, b.y), p3 = __floats2bfloat162_rn(b.z, b.w);
+    uint4 r;
+    r.x = *reinterpret_cast<uint32_t*>(&p0);
+    r.y = *reinterpret_cast<uint32_t*>(&p1);
+    r.z = *reinterpret_cast<uint32_t*>(&p2);
+    r.w = *reinterpret_cast<uint32_t*>(&p3);
+    return r;
+}
+
+// Staging unit u of a 128 x K tile of A: 8 consecutive k (32 bytes of fp32) of one
+// row. With t = u / 8, the unit is k-block t mod (K/8) of row 8 (t div (K/8)) + u mod 8,
+// which puts it at byte u * 16 of the canonical K-major layout: a warp's 32 units fill
+// 512 contiguous bytes of shared memory (no bank conflicts) and read 128 contiguous
+// bytes from each of 8 rows (whole sectors) when K >= 32.
+template <int K>
+__device__ __forceinline__ void unit_row_k(int u, int& r, int& k) {
+    const int t = u >> 3;
+    r = (t / (K / 8)) * 8 + (u & 7);
+    k = (t % (K / 8)) * 8;
+}
+
+template <int K>
+__device__ __forceinline__ void load_unit(const float* __restrict__ A, int lda, int M, int m0, int u, float4& lo,
+                                          float4& hi) {
+    int r, k;
+    unit_row_k<K>(u, r, k);
+    if (m0 + r < M) {
+        const float4* p = reinterpret_cast<const float4*>(A + static_cast<long long>(m0 + r) * lda + k);
+        lo = __ldg(p);
+        hi = __ldg(p + 1);
+    } else {
+        lo = hi = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
 template <int N, int K>
 struct TcShape {
     static_assert(N == 64 || N == 128, "N is 64 or 128");
@@ -77,7 +137,12 @@ struct TcShape {
     static constexpr int kM = 128;
     static constexpr int kABytes = kM * K * 2;
     static constexpr int kBBytes = N * K * 2;
-    static constexpr int kSmem = kABytes + kBBytes + 64 + 128;  // + mbarrier, TMEM address slot, alignment
+    // epilogue staging (4 warps x 32 rows x 16 floats) in the A buffer, or after B when
+    // the A buffer is smaller
+    static constexpr int kStageBytes = 4 * 32 * 16 * 4;
+    static constexpr int kStageOffset = kABytes >= kStageBytes ? 0 : kABytes + kBBytes;
+    static constexpr int kExtra = kABytes >= kStageBytes ? 0 : kStageBytes;
+    static constexpr int kSmem = kABytes + kBBytes + kExtra + 64 + 128;  // + mbarrier, TMEM slot, alignment
     static constexpr int kCols = N;                              // TMEM columns (a power of 2 >= 32)
 };
 
@@ -91,13 +156,30 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, const float* __restrict_
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     unsigned char* sA = smem;
     unsigned char* sB = smem + S::kABytes;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + S::kBBytes);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + S::kBBytes + S::kExtra);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    for (int e = tid; e < N * K; e += 128) {
-        const int n = e / K, k = e - n * K;
-        *reinterpret_cast<__nv_bfloat16*>(sB + kmajor_offset<K>(n, k)) = B[static_cast<long long>(k) * sbk + n * sbn];
+    // B in pieces of 8 consecutive k of one column n (16 bytes at kmajor_offset(n, k)):
+    // lanes take consecutive n, so the loads are contiguous when n is the contiguous
+    // index (sbn == 1) and each piece is one 16-byte load when k is (sbk == 1).
+#pragma unroll 4
+    for (int e = tid; e < N * (K / 8); e += 128) {
+        const int n = e % N, k = (e / N) * 8;
+        uint4 piece;
+        if (sbk == 1) {
+            piece = *reinterpret_cast<const uint4*>(B + static_cast<long long>(n) * sbn + k);
+        } else {
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat16 lo = B[static_cast<long long>(k + 2 * j) * sbk + static_cast<long long>(n) * sbn];
+                const __nv_bfloat16 hi = B[static_cast<long long>(k + 2 * j + 1) * sbk + static_cast<long long>(n) * sbn];
+                w[j] = static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+            }
+            piece = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        *reinterpret_cast<uint4*>(sB + kmajor_offset<K>(n, k)) = piece;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -116,18 +198,27 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, const float* __restrict_
     const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB), bar = smem_u32(mbar);
     uint32_t phase = 0;
     bool failed = false;
+    // A tile staging: each thread owns units tid + 128 i (i < K/8), loaded in batches of
+    // kUB units; the first batch of the next tile is loaded while this tile's MMAs and
+    // epilogue run.
+    constexpr int kPer = K / 8, kUB = kPer < 8 ? kPer : 8;
+    float4 buf[2 * kUB];
+    if (blockIdx.x * S::kM < M) {
+#pragma unroll
+        for (int i = 0; i < kUB; ++i) load_unit<K>(A, lda, M, blockIdx.x * S::kM, tid + 128 * i, buf[2 * i], buf[2 * i + 1]);
+    }
     for (int tile = blockIdx.x; tile * S::kM < M && !failed; tile += gridDim.x) {
         const int m0 = tile * S::kM;
-        // A tile: fp32 -> bf16, four consecutive k per thread step (8 bytes into one core row)
-        for (int q = tid; q < S::kM * (K / 4); q += 128) {
-            const int r = q / (K / 4), k4 = (q - r * (K / 4)) * 4;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (m0 + r < M) v = *reinterpret_cast<const float4*>(A + static_cast<long long>(m0 + r) * lda + k4);
-            __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
-            uint2 packed;
-            packed.x = *reinterpret_cast<uint32_t*>(&lo);
-            packed.y = *reinterpret_cast<uint32_t*>(&hi);
-            *reinterpret_cast<uint2*>(sA + kmajor_offset<K>(r, k4)) = packed;
+#pragma unroll
+        for (int b = 0; b < kPer / kUB; ++b) {
+            if (b > 0) {
+#pragma unroll
+                for (int i = 0; i < kUB; ++i)
+                    load_unit<K>(A, lda, M, m0, tid + 128 * (b * kUB + i), buf[2 * i], buf[2 * i + 1]);
+            }
+#pragma unroll
+            for (int i = 0; i < kUB; ++i)
+                *reinterpret_cast<uint4*>(sA + (tid + 128 * (b * kUB + i)) * 16) = pack8(buf[2 * i], buf[2 * i + 1]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -146,12 +237,23 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, const float* __restrict_
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                          : "memory");
         }
+        const int next = tile + gridDim.x;
+        if (next * S::kM < M) {
+#pragma unroll
+            for (int i = 0; i < kUB; ++i) load_unit<K>(A, lda, M, next * S::kM, tid + 128 * i, buf[2 * i], buf[2 * i + 1]);
+        }
         const bool ok = mbar_wait(bar, phase, kWaitLimit);
         failed = __syncthreads_or(!ok) != 0;
         phase ^= 1u;
         if (failed) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int row = m0 + warp * 32 + lane;
+        // Epilogue: each warp takes its 32 rows 16 columns at a time from TMEM (one row
+        // per lane), applies bias / relu and passes them through shared memory (the A
+        // buffer, free once the MMAs are done; 16-float rows with the float4 slots XOR-ed
+        // by (row / 2) mod 4, which keeps both the row-wise writes and the column-wise
+        // reads free of bank conflicts), so that a store instruction writes 64 contiguous
+        // bytes of each of 8 rows instead of 16 bytes of each of 32.
+        float* stg = reinterpret_cast<float*>(sA + S::kStageOffset) + warp * 32 * 16;
 #pragma unroll
         for (int c0 = 0; c0 < N; c0 += 16) {
             uint32_t v[16];
@@ -162,22 +264,28 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, const float* __restrict_
                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
                 : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < M) {
-                float* out = C + static_cast<long long>(row) * ldc + c0;
 #pragma unroll
-                for (int j = 0; j < 16; j += 4) {
-                    float4 o;
-                    float* f = &o.x;
+            for (int q = 0; q < 4; ++q) {
+                float4 o;
+                float* f = &o.x;
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        float t = __uint_as_float(v[j + e]);
-                        if (bias) t += bias[c0 + j + e];
-                        if (relu) t = fmaxf(t, 0.f);
-                        f[e] = t;
-                    }
-                    *reinterpret_cast<float4*>(out + j) = o;
+                for (int e = 0; e < 4; ++e) {
+                    float t = __uint_as_float(v[4 * q + e]);
+                    if (bias) t += bias[c0 + 4 * q + e];
+                    if (relu) t = fmaxf(t, 0.f);
+                    f[e] = t;
                 }
+                *reinterpret_cast<float4*>(stg + lane * 16 + 4 * (q ^ ((lane >> 1) & 3))) = o;
             }
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int rr = 8 * i + (lane >> 2), q = lane & 3;
+                const float4 o = *reinterpret_cast<const float4*>(stg + rr * 16 + 4 * (q ^ ((rr >> 1) & 3)));
+                const int row = m0 + warp * 32 + rr;
+                if (row < M) *reinterpret_cast<float4*>(C + static_cast<long long>(row) * ldc + c0 + 4 * q) = o;
+            }
+            __syncwarp();
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
@@ -188,6 +296,164 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, const float* __restrict_
         mbar_wait(bar, phase ^ 1u, kWaitLimit);
         __syncthreads();
     }
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::kCols));
+}
+
+// ------------------------------------------------------------ weight gradient
+//
+// part[z][f * 64 + n] = sum over the nodes k of slice z of X[k][f] dZ[k][n]: the
+// weight gradient dW = X^T dZ of a 128-wide layer input (f < 128) against the 64
+// channels of dZ, over the node slice [z chunk, min(rows, (z + 1) chunk)). The fixed
+// slices are summed afterwards in slice order, so the result does not depend on
+// timing.
+//
+// The node index is the MMA's K: A = X^T (128 x nodes) and B = dZ (nodes x 64) are
+// both MN-major, so one 32-byte piece of a row of X or dZ (8 features or channels of
+// one node) becomes one 16-byte core row. A stage holds 64 nodes: A 16 KB (core
+// (feature block i, node block j) at j 2048 + i 128) and B 8 KB (j 1024 + i 128);
+// with unit u = thread + 128 v, piece u lands at byte u * 16 (linear, no bank
+// conflicts). Two stages alternate: the threads stage one while the tensor core
+// works on the other; an mbarrier per stage says when its MMAs have read it.
+struct WgShape {
+    static constexpr int kNodes = 64;                      // nodes per stage
+    static constexpr int kABytes = 128 * kNodes * 2;       // X^T stage
+    static constexpr int kBBytes = kNodes * 64 * 2;        // dZ stage
+    static constexpr int kStage = kABytes + kBBytes;
+    static constexpr int kSmem = 2 * kStage + 64 + 128;    // + 2 mbarriers, TMEM slot, alignment
+    static constexpr int kCols = 64;                       // TMEM columns: 128 lanes x 64 fp32
+};
+
+template <int F>
+__global__ void __launch_bounds__(128) k_wgrad_tc(int rows, int chunk, const float* __restrict__ X, int ldx,
+                                                  const float* __restrict__ dZ, float* __restrict__ part,
+                                                  unsigned int* __restrict__ err) {
+    static_assert(F == 128, "the layer input is 128 wide");
+    using S = WgShape;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 2 * S::kStage);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k0 = blockIdx.x * chunk, k1 = min(rows, k0 + chunk);
+    const int stages = k1 > k0 ? (k1 - k0 + S::kNodes - 1) / S::kNodes : 0;
+    float* out = part + static_cast<long long>(blockIdx.x) * (128 * 64);
+    if (stages == 0) {
+        for (int e = tid; e < 128 * 64; e += 128) out[e] = 0.f;
+        return;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(S::kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = instr_desc_bf16_mn(128, 64);
+    bool failed = false;
+    int issued = 0;
+    for (int st = 0; st < stages; ++st) {
+        const int b = st & 1, nb = k0 + st * S::kNodes;
+        unsigned char* sA = smem + b * S::kStage;
+        unsigned char* sB = sA + S::kABytes;
+        // X pieces: 1,024 per stage, 8 per thread (node block u / 128, feature block
+        // (u / 8) mod 16, node u mod 8); dZ pieces: 512 per stage, 4 per thread (node
+        // block u / 64, channel block (u / 8) mod 8, node u mod 8). All 24 loads are
+        // issued before the wait for the buffer.
+        float4 xa[16], za[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+            const int u = tid + 128 * v, node = nb + (u >> 7) * 8 + (u & 7), f = ((u >> 3) & 15) * 8;
+            if (node < k1) {
+                const float4* p = reinterpret_cast<const float4*>(X + static_cast<long long>(node) * ldx + f);
+                xa[2 * v] = __ldg(p);
+                xa[2 * v + 1] = __ldg(p + 1);
+            } else {
+                xa[2 * v] = xa[2 * v + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int u = tid + 128 * v, node = nb + (u >> 6) * 8 + (u & 7), c = ((u >> 3) & 7) * 8;
+            if (node < k1) {
+                const float4* p = reinterpret_cast<const float4*>(dZ + static_cast<long long>(node) * 64 + c);
+                za[2 * v] = __ldg(p);
+                za[2 * v + 1] = __ldg(p + 1);
+            } else {
+                za[2 * v] = za[2 * v + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+        // the MMAs of stage st - 2 read this buffer: wait for their commit
+        bool ok = true;
+        if (st >= 2) ok = mbar_wait(smem_u32(mbar + b), static_cast<uint32_t>(((st - 2) >> 1) & 1), kWaitLimit);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) *reinterpret_cast<uint4*>(sA + (tid + 128 * v) * 16) = pack8(xa[2 * v], xa[2 * v + 1]);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) *reinterpret_cast<uint4*>(sB + (tid + 128 * v) * 16) = pack8(za[2 * v], za[2 * v + 1]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        failed = __syncthreads_or(!ok) != 0;
+        if (failed) break;
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+            for (int s = 0; s < S::kNodes / 16; ++s) {
+                const uint64_t da = smem_desc(a0 + s * 2 * 2048, 2048, 128);
+                const uint64_t db = smem_desc(b0 + s * 2 * 1024, 1024, 128);
+                const uint32_t accumulate = (st > 0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(mbar + b))
+                         : "memory");
+        }
+        issued = st + 1;
+    }
+    if (!failed) {
+        // the last commit completes after every MMA before it
+        const int last = stages - 1;
+        const bool ok = mbar_wait(smem_u32(mbar + (last & 1)), static_cast<uint32_t>((last >> 1) & 1), kWaitLimit);
+        failed = __syncthreads_or(!ok) != 0;
+    }
+    if (!failed) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        float* row = out + (warp * 32 + lane) * 64;
+#pragma unroll
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            uint32_t v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                *reinterpret_cast<float4*>(row + c0 + 4 * q) =
+                    make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                                __uint_as_float(v[4 * q + 3]));
+        }
+    } else {
+        // let the MMAs already committed finish before TMEM is freed (bounded)
+        if (tid == 0) atomicOr(err, 1u);
+        for (int b = 0; b < 2; ++b) {
+            const int st = issued - 1 - ((issued - 1 - b) & 1);   // last stage issued on buffer b
+            if (st >= 0 && (st & 1) == b) mbar_wait(smem_u32(mbar + b), static_cast<uint32_t>((st >> 1) & 1), kWaitLimit);
+        }
+        __syncthreads();
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::kCols));
 }
 

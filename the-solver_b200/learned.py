@@ -26,17 +26,33 @@ def solve(engine, matrix, inst, eps, x0=None, y0=None, max_iterations=200_000, o
     return rc, x, y, res, time.perf_counter() - t
 
 
-def dataset(engine, matrix, members, eps, progress=None):
-    """(member, x*, y*, final primal weight) for every member whose PDLP solve converged."""
-    out = []
-    for k, inst in enumerate(members):
+def dataset(engine, matrix, members, eps, progress=None, workers=1):
+    """(member, x*, y*, final primal weight) for every member whose PDLP solve converged,
+    in member order. With workers > 1 the solves run concurrently from that many host
+    threads: each thread's calls go to its own stream with their own buffers (the
+    matrix is only read), and every solve is deterministic, so the pairs are the same
+    as with one worker."""
+    import sys
+
+    def one(inst):
         rc, x, y, res, _ = solve(engine, matrix, inst, eps)
-        if rc == 0 and res["status"] == 0:
-            out.append((inst, x, y, res["primal_weight"]))
-        if progress and (k + 1) % progress == 0:
-            import sys
-            print(f"solved {k + 1} / {len(members)}", file=sys.stderr, flush=True)
-    return out
+        return (inst, x, y, res["primal_weight"]) if rc == 0 and res["status"] == 0 else None
+
+    results = []
+    if workers <= 1:
+        for k, inst in enumerate(members):
+            results.append(one(inst))
+            if progress and (k + 1) % progress == 0:
+                print(f"solved {k + 1} / {len(members)}", file=sys.stderr, flush=True)
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(max_workers=workers) as pool:
+            for k, r in enumerate(pool.map(one, members)):
+                results.append(r)
+                if progress and (k + 1) % progress == 0:
+                    print(f"solved {k + 1} / {len(members)}", file=sys.stderr, flush=True)
+    return [r for r in results if r is not None]
 
 
 def dual_scale(data):
@@ -121,6 +137,8 @@ def main(argv=None):
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--train-eps", type=float, default=1e-6)
     ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--workers", type=int, default=1, help="concurrent solves while making the training set")
+    ap.add_argument("--eval-seed", type=int, default=900_000, help="first seed of the evaluation members")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only time this many training steps (zero targets, no PDLP solves) and one prediction")
     a = ap.parse_args(argv)
@@ -143,7 +161,7 @@ def main(argv=None):
         return
     t = time.perf_counter()
     data = dataset(engine, matrix, [instances.lp_family_member(base, 1000 + s) for s in range(a.train)], a.train_eps,
-                   progress=50)
+                   progress=50, workers=a.workers)
     t_data = time.perf_counter() - t
     net = engine.Gnn(seed=a.seed, y_scale=dual_scale(data))
     t = time.perf_counter()
@@ -152,8 +170,8 @@ def main(argv=None):
     mean_x = np.mean([d[1] for d in data], axis=0)
     mean_y = np.mean([d[2] for d in data], axis=0)
     omega = learned_weight(data)
-    rows = evaluate(engine, net, matrix, [instances.lp_family_member(base, 900_000 + s) for s in range(a.eval)], a.eps,
-                    mean_x, mean_y, omega)
+    rows = evaluate(engine, net, matrix, [instances.lp_family_member(base, a.eval_seed + s) for s in range(a.eval)],
+                    a.eps, mean_x, mean_y, omega)
     avg = lambda k: float(np.mean([r[k] for r in rows])) if rows else None
     out = dict(workload=f"lp_family: m={a.m}, n={a.n}, {a.per_col} per column, seed {a.seed}",
                nnz=int(base["ptr"][-1]), eps=a.eps, train_members=len(data), train_eps=a.train_eps,
