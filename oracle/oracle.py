@@ -45,6 +45,8 @@ def load(name: str) -> C.CDLL:
                 "ref_scaling": os.path.join(HERE, "_ref", "libsihps_scaling_ref.so"),
                 "ref_pdlp": os.path.join(HERE, "_ref", "libsihps_pdlp_ref.so"),
                 "ref_hooked": os.path.join(HERE, "_ref", "libsankhya_ref_hooked.so"),
+                "ref_lp": os.path.join(HERE, "_ref", "libsihps_lp_ref.so"),
+                "ref_lp_hooked": os.path.join(HERE, "_ref", "libsihps_lp_hooked.so"),
                 "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so")}[name]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")
@@ -295,6 +297,54 @@ def ref_gpupdlp(inst, eps=1e-8, max_iterations=500000, restart_period=64, power_
     if rc != 0:
         raise RuntimeError("reference GpuPdlp failed")
     return x, {k: getattr(st, k) for k, _ in RefPdlpStats._fields_}
+
+
+class RefLpOptions(C.Structure):
+    """RefLpOptions of ref_lpsolver_shim.cpp (a subset of sihps::LpSolverOptions)."""
+    _fields_ = [("method", C.c_int), ("use_presolve", C.c_int), ("hybrid_row_threshold", C.c_int),
+                ("pdlp_max_iterations", C.c_int), ("pdlp_eps", C.c_double), ("pdlp_time_limit", C.c_double),
+                ("hybrid_first_order_eps", C.c_double), ("hybrid_first_order_budget", C.c_double),
+                ("hybrid_simplex_budget", C.c_double)]
+
+
+class RefLpResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("used_first_order", C.c_int),
+                ("first_order_fallback_used", C.c_int), ("pdlp_converged", C.c_int), ("pdlp_iterations", C.c_int),
+                ("objective", C.c_double), ("primal_residual", C.c_double), ("pdlp_relative_gap", C.c_double),
+                ("solve_seconds", C.c_double)]
+
+
+LP_SIMPLEX, LP_FIRST_ORDER, LP_HYBRID = 0, 1, 2
+LP_STATUS = ("OPTIMAL", "INFEASIBLE", "UNBOUNDED", "ITERATION_LIMIT", "NUMERICAL_FAILURE")
+
+
+def ref_solve_lp(inst, method=LP_SIMPLEX, hooked=False, **opts):
+    """The reference C++ core's sihps::solve_lp (src/lp/LpSolver.cpp:126-334) on the
+    instance: (x, result dict). `hooked` selects the build whose run_first_order is the
+    integration block calling the engine; otherwise FIRST_ORDER runs the reference's own
+    GpuPdlp. Keyword options are RefLpOptions fields; the rest keep the core's defaults.
+    SIMPLEX runs on the CPU; FIRST_ORDER and HYBRID need a GPU."""
+    lib = load("ref_lp_hooked" if hooked else "ref_lp")
+    o = RefLpOptions()
+    lib.ref_lp_default_options(C.byref(o))
+    o.method = method
+    for k, v in opts.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    keep = _Keep()
+    r = RefLpResult()
+    x = np.zeros(inst["n"])
+    fn = lib.ref_solve_lp
+    fn.restype = C.c_int
+    rc = fn(C.c_int(inst["m"]), C.c_int(inst["n"]), C.c_int(int(inst["ptr"][-1])), _p(keep.i(inst["ptr"]), iptr),
+            _p(keep.i(inst["idx"]), iptr), _p(keep.d(inst["val"])), _p(keep.d(inst["c"])), _p(keep.d(inst["cl"])),
+            _p(keep.d(inst["cu"])), _p(keep.d(inst["rl"])), _p(keep.d(inst["ru"])), C.byref(o), _p(x), C.byref(r))
+    if rc != 0:
+        raise RuntimeError("reference solve_lp threw")
+    out = {k: getattr(r, k) for k, _ in RefLpResult._fields_}
+    out["status_name"] = LP_STATUS[out["status"]] if 0 <= out["status"] < len(LP_STATUS) else str(out["status"])
+    return x, out
 
 
 class RefCudaCsr(C.Structure):

@@ -5,8 +5,8 @@ reference's code and this library's C ABI:
 
 - the sihps caller: `run_first_order` (src/lp/LpSolver.cpp:62-99) replaced by one
   sankhya_b200_pdlp_solve call, checked with g++ -fsyntax-only against LpProblem,
-  CSRMatrix, PdlpParams and PdlpStats. Linking and running need the rest of the C++
-  core, which its own CMake project builds; that is not run here;
+  CSRMatrix, PdlpParams and PdlpStats (oracle/hooked_lpsolver.py links the spliced
+  core and tests/test_gpu_lpsolver_first_order.py runs it);
 - the MILP batch caller: the node-relaxation block wrapped in a function appended to
   c/src/sk_milp.c, where the `milp` driver struct it reads (M->m, M->lp_opt) is
   defined, checked with gcc -fsyntax-only."""
@@ -38,12 +38,8 @@ def _milp_block():
 
 
 def _spliced(text, block):
-    start = text.index("bool run_first_order(const LpProblem& target")
-    end = text.index("\n}\n", start) + 3
-    out = text[:start] + block + text[end:]
-    anchor = '#include "Scaling.hpp"\n'
-    assert anchor in out
-    return out.replace(anchor, anchor + '#include "sankhya_b200.h"\n', 1)
+    import hooked_lpsolver
+    return hooked_lpsolver.spliced(text, block)
 
 
 def _compile(ref, source):
