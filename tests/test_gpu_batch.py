@@ -32,6 +32,18 @@ def test_uneven_batch_matches_separate_solves(engine, oracle, instances):
     assert len({r["iterations"] for r in res}) > 10    # ... each at its own iteration
 
 
+def test_config3a_size_range_matches_separate_solves(engine, oracle, instances):
+    """64 LPs drawn with config 3a's recipe over its whole size range (m log-uniform in
+    [50, 5,000], n = 2m, 4-8 per column; 0.86M nonzeros in all): bit-identical iterates
+    and stopping iterations against separate oracle runs, most LPs stopping at their own
+    gate and some at the iteration limit."""
+    lps = instances.lp_batch_uneven(35, 64, 50, 5000)
+    assert max(lp["m"] for lp in lps) > 4000
+    res = _check_against_oracle(engine, oracle, lps, 4000, ptol=3e-3, dtol=3e-3)
+    assert 40 <= sum(r["status"] == 0 for r in res) < 64
+    assert len({r["iterations"] for r in res}) > 30
+
+
 def test_iteration_limit_not_multiple_of_check(engine, oracle, instances):
     lps = instances.lp_batch_uneven(32, 12, 30, 120)
     res = _check_against_oracle(engine, oracle, lps, 137, ptol=1e-12, dtol=1e-12)
