@@ -79,6 +79,21 @@ def test_diagonal_and_sparse_qp_bit_exact(engine, oracle, instances):
     assert abs(r["objective"] - r2["objective"]) <= 1e-12 * (1 + abs(r2["objective"]))
 
 
+def test_qp_config2_within_tolerance(engine, oracle, instances):
+    """The config-2 QP itself (n = 200,000, m = 100,000, 2M nonzeros in A, explicit
+    Q = D + L L^T with 1.4M): 40 fixed-step iterations of the diagonal-proximal and
+    the sparse-Hessian entry points against the oracle. Some rows of A are longer than
+    32 entries (warp-tree sums), so the comparison is at 1e-9 relative."""
+    inst = instances.qp_config2(2)
+    s = fixed_settings(engine, max_iterations=40, check_every=20, tau=0.005, sigma=0.5)
+    for kw in (dict(qdiag=inst["qdiag"]), dict(hessian=True)):
+        (rc, x, y, r), (rc2, x2, y2, r2) = run_both(engine, oracle, inst, s, **kw)
+        assert rc == rc2 == 0, kw.keys()
+        assert np.abs(x - x2).max() <= 1e-9 * (1 + np.abs(x2).max()), kw.keys()
+        assert np.abs(y - y2).max() <= 1e-9 * (1 + np.abs(y2).max()), kw.keys()
+        assert abs(r["objective"] - r2["objective"]) <= 1e-9 * (1 + abs(r2["objective"]))
+
+
 def test_converges_like_the_oracle(engine, oracle, instances):
     """Same stopping iteration and status when the gates fire."""
     inst = instances.lp_uniform(4, 50, 120, 3)
