@@ -27,6 +27,7 @@
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -596,9 +597,31 @@ bool tc_fits(const void* a, int lda, const void* c, int ldc) {
            lda % 4 == 0 && ldc % 4 == 0;
 }
 
+// K = 64 / 128: the cp.async-pipelined kernel, one CTA per SM (its shared memory).
+template <int N, int K, int ST>
+void gemm_tc_pipe(SankhyaB200Gnn* s, cudaStream_t st, int M, const float* A, int lda, const __nv_bfloat16* B, int sbk,
+                  int sbn, const float* bias, int relu, float* C, int ldc) {
+    using S = tc::TcPipeShape<N, K, ST>;
+    const void* fn = reinterpret_cast<const void*>(&tc::k_gemm_tc_pipe<N, K, ST>);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmem);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, S::kThreads, S::kSmem);
+    const int tiles = (M + S::kM - 1) / S::kM;
+    const int grid = std::max(1, std::min(tiles, s->sms * std::max(1, per_sm)));
+    tc::k_gemm_tc_pipe<N, K, ST><<<grid, S::kThreads, S::kSmem, st>>>(M, A, lda, B, sbk, sbn, bias, relu, C, ldc,
+                                                                       s->tc_flag.as<unsigned int>());
+}
+
 template <int N, int K>
 void gemm_tc(SankhyaB200Gnn* s, cudaStream_t st, int M, const float* A, int lda, const __nv_bfloat16* B, int sbk,
              int sbn, const float* bias, int relu, float* C, int ldc) {
+    if constexpr (K == 128) {
+        gemm_tc_pipe<N, K, 2>(s, st, M, A, lda, B, sbk, sbn, bias, relu, C, ldc);
+        return;
+    } else if constexpr (K == 64) {
+        gemm_tc_pipe<N, K, 3>(s, st, M, A, lda, B, sbk, sbn, bias, relu, C, ldc);
+        return;
+    }
     using S = tc::TcShape<N, K>;
     const void* fn = reinterpret_cast<const void*>(&tc::k_gemm_tc<N, K>);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmem);
@@ -652,15 +675,17 @@ void gemm_weight_grad(SankhyaB200Gnn* s, cudaStream_t st, int rows, const float*
         return;
     }
     if (K == kX && tc_fits(X, ldx, dz, kH)) {
-        // tensor-core path: slices of a whole number of 64-node stages, at most 2 per SM
-        const int stage = tc::WgShape::kNodes;
-        const int want = std::max(1, std::min(148 * 2, (rows + 255) / 256));
-        const int chunk = ((rows + want - 1) / want + stage - 1) / stage * stage;
+        // tensor-core path: one slice (a whole number of 64-node stages) per resident CTA
+        using W = tc::WgPipeShape<3>;
+        const void* fn = reinterpret_cast<const void*>(&tc::k_wgrad_tc_pipe<kX, 3>);
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, W::kSmem);
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, W::kThreads, W::kSmem);
+        const int want = std::max(1, std::min({148 * 2, s->sms * std::max(1, per_sm), (rows + W::kNodes - 1) / W::kNodes}));
+        const int chunk = ((rows + want - 1) / want + W::kNodes - 1) / W::kNodes * W::kNodes;
         const int slices = (rows + chunk - 1) / chunk;
-        const void* fn = reinterpret_cast<const void*>(&tc::k_wgrad_tc<kX>);
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::WgShape::kSmem);
-        tc::k_wgrad_tc<kX><<<slices, 128, tc::WgShape::kSmem, st>>>(rows, chunk, X, ldx, dz, s->part,
-                                                                 s->tc_flag.as<unsigned int>());
+        tc::k_wgrad_tc_pipe<kX, 3><<<slices, W::kThreads, W::kSmem, st>>>(rows, chunk, X, ldx, dz, s->part,
+                                                                           s->tc_flag.as<unsigned int>());
         sum_slices(K * kH, slices, static_cast<long long>(K) * kH, s->part, out, st);
         return;
     }

@@ -299,6 +299,207 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, const float* __restrict_
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::kCols));
 }
 
+// ------------------------------------------------------ layer GEMM, pipelined
+//
+// The same product for K in {64, 128}, fed by cp.async instead of register-staged
+// loads, so that a CTA keeps ST - 1 fp32 tiles (64 or 32 KB each) in flight while it
+// converts, multiplies and writes back the current one:
+//   - a tile's 16-byte chunks (row r, chunk c) are copied to row r of an fp32 stage
+//     at chunk position c XOR (r mod 8) (rows past M are zero-filled by a source size
+//     of 0 and read nothing);
+//   - the threads convert the stage to bf16 in the canonical K-major layout, piece u
+//     (8 k of one row, as in k_gemm_tc) at byte 16 u: the 8 rows a warp phase reads
+//     sit at 8 different chunk positions, so the reads are free of bank conflicts,
+//     and so are the linear writes;
+//   - thread 0 issues the K/16 MMAs, and 8 warps run the epilogue: warp w reads TMEM
+//     lanes 32 (w mod 4) (the quarter a warp may access) for column half w / 4.
+// One CTA per SM (its shared memory), persistent over the 128-row tiles.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int Pending>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(Pending) : "memory");
+}
+
+template <int N, int K, int ST>
+struct TcPipeShape {
+    static_assert(N == 64 || N == 128, "N is 64 or 128");
+    static_assert(K == 64 || K == 128, "K is 64 or 128");
+    static_assert(ST >= 2 && ST <= 4, "2 to 4 stages");
+    static constexpr int kThreads = 256;
+    static constexpr int kM = 128;
+    static constexpr int kChunks = K / 4;                 // 16-byte chunks per fp32 row
+    static constexpr int kStageBytes = kM * K * 4;        // one fp32 tile
+    static constexpr int kABytes = kM * K * 2;            // bf16 canonical A
+    static constexpr int kBBytes = N * K * 2;             // bf16 canonical B
+    static constexpr int kEpiBytes = 8 * 32 * 16 * 4;     // 8 warps x 32 rows x 16 floats
+    static constexpr int kSmem = ST * kStageBytes + kABytes + kBBytes + kEpiBytes + 64 + 128;
+    static constexpr int kCols = N;
+};
+
+template <int N, int K, int ST>
+__global__ void __launch_bounds__(256) k_gemm_tc_pipe(int M, const float* __restrict__ A, int lda,
+                                                      const __nv_bfloat16* __restrict__ B, int sbk, int sbn,
+                                                      const float* __restrict__ bias, int relu, float* __restrict__ C,
+                                                      int ldc, unsigned int* __restrict__ err) {
+    using S = TcPipeShape<N, K, ST>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    unsigned char* stages = smem;
+    unsigned char* sA = smem + ST * S::kStageBytes;
+    unsigned char* sB = sA + S::kABytes;
+    float* sE = reinterpret_cast<float*>(sB + S::kBBytes);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + S::kBBytes + S::kEpiBytes);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles = (M + S::kM - 1) / S::kM;
+
+    // fp32 tile `tile` into stage `s` (an empty group past the last tile keeps the
+    // group count uniform)
+    auto issue = [&](int tile, int s) {
+        if (tile < tiles) {
+            const int m0 = tile * S::kM;
+            const uint32_t base = smem_u32(stages + s * S::kStageBytes);
+#pragma unroll 4
+            for (int q = tid; q < S::kM * S::kChunks; q += S::kThreads) {
+                const int r = q / S::kChunks, c = q - r * S::kChunks;
+                const bool live = m0 + r < M;
+                const float* src = A + static_cast<long long>(live ? m0 + r : 0) * lda + c * 4;
+                cp_async16(base + r * (K * 4) + ((c ^ (r & 7)) << 4), src, live ? 16 : 0);
+            }
+        }
+        cp_async_commit();
+    };
+    const int t0 = blockIdx.x;
+#pragma unroll
+    for (int s = 0; s < ST - 1; ++s) issue(t0 + s * gridDim.x, s);
+
+    // B pieces as in k_gemm_tc
+#pragma unroll 4
+    for (int e = tid; e < N * (K / 8); e += S::kThreads) {
+        const int n = e % N, k = (e / N) * 8;
+        uint4 piece;
+        if (sbk == 1) {
+            piece = *reinterpret_cast<const uint4*>(B + static_cast<long long>(n) * sbn + k);
+        } else {
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat16 lo = B[static_cast<long long>(k + 2 * j) * sbk + static_cast<long long>(n) * sbn];
+                const __nv_bfloat16 hi = B[static_cast<long long>(k + 2 * j + 1) * sbk + static_cast<long long>(n) * sbn];
+                w[j] = static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+            }
+            piece = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        *reinterpret_cast<uint4*>(sB + kmajor_offset<K>(n, k)) = piece;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(S::kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = instr_desc_bf16(S::kM, N);
+    const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB), bar = smem_u32(mbar);
+    uint32_t phase = 0;
+    bool failed = false;
+    const int quarter = warp & 3, half = warp >> 2;
+    float* stg = sE + warp * 32 * 16;
+    int i = 0;
+    for (int tile = t0; tile < tiles; tile += gridDim.x, ++i) {
+        const int m0 = tile * S::kM, s = i % ST;
+        // the stage converted in the previous iteration takes tile i + ST - 1
+        issue(tile + (ST - 1) * gridDim.x, (i + ST - 1) % ST);
+        cp_async_wait<ST - 1>();
+        __syncthreads();
+        const unsigned char* st = stages + s * S::kStageBytes;
+#pragma unroll
+        for (int v = 0; v < K / 16; ++v) {
+            const int u = tid + S::kThreads * v;
+            int r, k;
+            unit_row_k<K>(u, r, k);
+            const unsigned char* row = st + r * (K * 4);
+            const float4 lo = *reinterpret_cast<const float4*>(row + (((k >> 2) ^ (r & 7)) << 4));
+            const float4 hi = *reinterpret_cast<const float4*>(row + ((((k >> 2) + 1) ^ (r & 7)) << 4));
+            *reinterpret_cast<uint4*>(sA + u * 16) = pack8(lo, hi);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int k16 = 0; k16 < K / 16; ++k16) {
+                const uint64_t da = smem_desc(a_base + k16 * 256, 128, (K / 8) * 128);
+                const uint64_t db = smem_desc(b_base + k16 * 256, 128, (K / 8) * 128);
+                const uint32_t accumulate = k16 > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        const bool ok = mbar_wait(bar, phase, kWaitLimit);
+        failed = __syncthreads_or(!ok) != 0;
+        phase ^= 1u;
+        if (failed) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int c0 = half * (N / 2); c0 < (half + 1) * (N / 2); c0 += 16) {
+            uint32_t v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(c0)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float4 o;
+                float* f = &o.x;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    float t = __uint_as_float(v[4 * q + e]);
+                    if (bias) t += bias[c0 + 4 * q + e];
+                    if (relu) t = fmaxf(t, 0.f);
+                    f[e] = t;
+                }
+                *reinterpret_cast<float4*>(stg + lane * 16 + 4 * (q ^ ((lane >> 1) & 3))) = o;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int rr = 8 * j + (lane >> 2), q = lane & 3;
+                const float4 o = *reinterpret_cast<const float4*>(stg + rr * 16 + 4 * (q ^ ((rr >> 1) & 3)));
+                const int row = m0 + quarter * 32 + rr;
+                if (row < M) *reinterpret_cast<float4*>(C + static_cast<long long>(row) * ldc + c0 + 4 * q) = o;
+            }
+            __syncwarp();
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (failed) {
+        // the MMA may still be writing TMEM: wait for it (bounded) before freeing
+        if (tid == 0) atomicOr(err, 1u);
+        mbar_wait(bar, phase ^ 1u, kWaitLimit);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::kCols));
+}
+
 // ------------------------------------------------------------ weight gradient
 //
 // part[z][f * 64 + n] = sum over the nodes k of slice z of X[k][f] dZ[k][n]: the
@@ -452,6 +653,174 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(int rows, int chunk, const flo
         }
         __syncthreads();
     }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::kCols));
+}
+
+// The weight gradient fed by cp.async: each 64-node stage of X (32 KB) and dZ (16 KB)
+// is copied as 16-byte chunks into one of ST fp32 stages (chunk c of node row k at
+// position c XOR (k mod 8); nodes past the slice are zero-filled), converted into one
+// of two bf16 MN-major buffers (the layout of k_wgrad_tc) and multiplied; ST - 1
+// stages are in flight while the current one is converted. 256 threads, one CTA per
+// SM; the epilogue splits TMEM by lane quarter (warp mod 4) and column half (warp / 4).
+template <int ST>
+struct WgPipeShape {
+    static constexpr int kThreads = 256;
+    static constexpr int kNodes = 64;
+    static constexpr int kXBytes = kNodes * 128 * 4;      // fp32 X rows of a stage
+    static constexpr int kZBytes = kNodes * 64 * 4;       // fp32 dZ rows of a stage
+    static constexpr int kStage = kXBytes + kZBytes;
+    static constexpr int kABytes = 128 * kNodes * 2;      // bf16 X^T
+    static constexpr int kBBytes = kNodes * 64 * 2;       // bf16 dZ
+    static constexpr int kBuf = kABytes + kBBytes;
+    static constexpr int kSmem = ST * kStage + 2 * kBuf + 64 + 128;
+    static constexpr int kCols = 64;
+};
+
+template <int F, int ST>
+__global__ void __launch_bounds__(256) k_wgrad_tc_pipe(int rows, int chunk, const float* __restrict__ X, int ldx,
+                                                       const float* __restrict__ dZ, float* __restrict__ part,
+                                                       unsigned int* __restrict__ err) {
+    static_assert(F == 128, "the layer input is 128 wide");
+    using S = WgPipeShape<ST>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    unsigned char* stages = smem;
+    unsigned char* bufs = smem + ST * S::kStage;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(bufs + 2 * S::kBuf);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k0 = blockIdx.x * chunk, k1 = min(rows, k0 + chunk);
+    const int nst = k1 > k0 ? (k1 - k0 + S::kNodes - 1) / S::kNodes : 0;
+    float* out = part + static_cast<long long>(blockIdx.x) * (128 * 64);
+    if (nst == 0) {
+        for (int e = tid; e < 128 * 64; e += S::kThreads) out[e] = 0.f;
+        return;
+    }
+    auto issue = [&](int st) {
+        if (st < nst) {
+            const int nb = k0 + st * S::kNodes;
+            const uint32_t xs = smem_u32(stages + (st % ST) * S::kStage), zs = xs + S::kXBytes;
+#pragma unroll 4
+            for (int q = tid; q < S::kNodes * 32; q += S::kThreads) {   // X: 32 chunks per node
+                const int k = q >> 5, c = q & 31;
+                const bool live = nb + k < k1;
+                const float* src = X + static_cast<long long>(live ? nb + k : 0) * ldx + c * 4;
+                cp_async16(xs + k * 512 + ((c ^ (k & 7)) << 4), src, live ? 16 : 0);
+            }
+#pragma unroll 4
+            for (int q = tid; q < S::kNodes * 16; q += S::kThreads) {   // dZ: 16 chunks per node
+                const int k = q >> 4, c = q & 15;
+                const bool live = nb + k < k1;
+                const float* src = dZ + static_cast<long long>(live ? nb + k : 0) * 64 + c * 4;
+                cp_async16(zs + k * 256 + ((c ^ (k & 7)) << 4), src, live ? 16 : 0);
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int st = 0; st < ST - 1; ++st) issue(st);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(S::kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = instr_desc_bf16_mn(128, 64);
+    bool failed = false;
+    int issued = 0;
+    for (int st = 0; st < nst; ++st) {
+        const int b = st & 1;
+        issue(st + ST - 1);
+        cp_async_wait<ST - 1>();
+        // the MMAs of stage st - 2 read buffer b: wait for their commit
+        bool ok = true;
+        if (st >= 2) ok = mbar_wait(smem_u32(mbar + b), static_cast<uint32_t>(((st - 2) >> 1) & 1), kWaitLimit);
+        failed = __syncthreads_or(!ok) != 0;
+        if (failed) break;
+        const unsigned char* xs = stages + (st % ST) * S::kStage;
+        const unsigned char* zs = xs + S::kXBytes;
+        unsigned char* sA = bufs + b * S::kBuf;
+        unsigned char* sB = sA + S::kABytes;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {   // X^T pieces (k_wgrad_tc numbering)
+            const int u = tid + S::kThreads * v, k = (u >> 7) * 8 + (u & 7), c = ((u >> 3) & 15) * 2;
+            const unsigned char* row = xs + k * 512;
+            const float4 lo = *reinterpret_cast<const float4*>(row + ((c ^ (k & 7)) << 4));
+            const float4 hi = *reinterpret_cast<const float4*>(row + (((c + 1) ^ (k & 7)) << 4));
+            *reinterpret_cast<uint4*>(sA + u * 16) = pack8(lo, hi);
+        }
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {   // dZ pieces
+            const int u = tid + S::kThreads * v, k = (u >> 6) * 8 + (u & 7), c = ((u >> 3) & 7) * 2;
+            const unsigned char* row = zs + k * 256;
+            const float4 lo = *reinterpret_cast<const float4*>(row + ((c ^ (k & 7)) << 4));
+            const float4 hi = *reinterpret_cast<const float4*>(row + (((c + 1) ^ (k & 7)) << 4));
+            *reinterpret_cast<uint4*>(sB + u * 16) = pack8(lo, hi);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+            for (int s = 0; s < S::kNodes / 16; ++s) {
+                const uint64_t da = smem_desc(a0 + s * 2 * 2048, 2048, 128);
+                const uint64_t db = smem_desc(b0 + s * 2 * 1024, 1024, 128);
+                const uint32_t accumulate = (st > 0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(mbar + b))
+                         : "memory");
+        }
+        issued = st + 1;
+    }
+    if (!failed) {
+        const int last = nst - 1;
+        const bool ok = mbar_wait(smem_u32(mbar + (last & 1)), static_cast<uint32_t>((last >> 1) & 1), kWaitLimit);
+        failed = __syncthreads_or(!ok) != 0;
+    }
+    if (!failed) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int quarter = warp & 3, half = warp >> 2;
+        float* row = out + (quarter * 32 + lane) * 64;
+#pragma unroll
+        for (int c0 = half * 32; c0 < half * 32 + 32; c0 += 16) {
+            uint32_t v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(c0)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                *reinterpret_cast<float4*>(row + c0 + 4 * q) =
+                    make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                                __uint_as_float(v[4 * q + 3]));
+        }
+    } else {
+        if (tid == 0) atomicOr(err, 1u);
+        for (int b = 0; b < 2; ++b) {
+            const int st = issued - 1 - ((issued - 1 - b) & 1);   // last stage committed on buffer b
+            if (st >= 0 && (st & 1) == b) mbar_wait(smem_u32(mbar + b), static_cast<uint32_t>((st >> 1) & 1), kWaitLimit);
+        }
+    }
+    cp_async_wait<0>();
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::kCols));
