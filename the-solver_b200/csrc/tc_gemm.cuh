@@ -22,7 +22,8 @@
 // operands are rounded to bf16 exactly as the mma.sync kernel rounds them; only
 // the fp32 accumulation order inside the tensor core differs.
 //
-// k_wgrad_tc (below) computes the weight gradients X^T dZ with both operands
+// k_gemm_tc_pipe (below) is the same product for K = 64 and 128 fed by cp.async stages,
+// and k_wgrad_tc_pipe computes the weight gradients X^T dZ with both operands
 // MN-major, summed over node slices in a fixed order.
 //
 // Descriptor bitfields follow CUTLASS's cute/arch/mma_sm100_desc.hpp
@@ -510,158 +511,15 @@ __global__ void __launch_bounds__(256) k_gemm_tc_pipe(int M, const float* __rest
 //
 // The node index is the MMA's K: A = X^T (128 x nodes) and B = dZ (nodes x 64) are
 // both MN-major, so one 32-byte piece of a row of X or dZ (8 features or channels of
-// one node) becomes one 16-byte core row. A stage holds 64 nodes: A 16 KB (core
-// (feature block i, node block j) at j 2048 + i 128) and B 8 KB (j 1024 + i 128);
-// with unit u = thread + 128 v, piece u lands at byte u * 16 (linear, no bank
-// conflicts). Two stages alternate: the threads stage one while the tensor core
-// works on the other; an mbarrier per stage says when its MMAs have read it.
-struct WgShape {
-    static constexpr int kNodes = 64;                      // nodes per stage
-    static constexpr int kABytes = 128 * kNodes * 2;       // X^T stage
-    static constexpr int kBBytes = kNodes * 64 * 2;        // dZ stage
-    static constexpr int kStage = kABytes + kBBytes;
-    static constexpr int kSmem = 2 * kStage + 64 + 128;    // + 2 mbarriers, TMEM slot, alignment
-    static constexpr int kCols = 64;                       // TMEM columns: 128 lanes x 64 fp32
-};
-
-template <int F>
-__global__ void __launch_bounds__(128) k_wgrad_tc(int rows, int chunk, const float* __restrict__ X, int ldx,
-                                                  const float* __restrict__ dZ, float* __restrict__ part,
-                                                  unsigned int* __restrict__ err) {
-    static_assert(F == 128, "the layer input is 128 wide");
-    using S = WgShape;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 2 * S::kStage);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int k0 = blockIdx.x * chunk, k1 = min(rows, k0 + chunk);
-    const int stages = k1 > k0 ? (k1 - k0 + S::kNodes - 1) / S::kNodes : 0;
-    float* out = part + static_cast<long long>(blockIdx.x) * (128 * 64);
-    if (stages == 0) {
-        for (int e = tid; e < 128 * 64; e += 128) out[e] = 0.f;
-        return;
-    }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(S::kCols));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
-    }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tslot;
-    const uint32_t idesc = instr_desc_bf16_mn(128, 64);
-    bool failed = false;
-    int issued = 0;
-    for (int st = 0; st < stages; ++st) {
-        const int b = st & 1, nb = k0 + st * S::kNodes;
-        unsigned char* sA = smem + b * S::kStage;
-        unsigned char* sB = sA + S::kABytes;
-        // X pieces: 1,024 per stage, 8 per thread (node block u / 128, feature block
-        // (u / 8) mod 16, node u mod 8); dZ pieces: 512 per stage, 4 per thread (node
-        // block u / 64, channel block (u / 8) mod 8, node u mod 8). All 24 loads are
-        // issued before the wait for the buffer.
-        float4 xa[16], za[8];
-#pragma unroll
-        for (int v = 0; v < 8; ++v) {
-            const int u = tid + 128 * v, node = nb + (u >> 7) * 8 + (u & 7), f = ((u >> 3) & 15) * 8;
-            if (node < k1) {
-                const float4* p = reinterpret_cast<const float4*>(X + static_cast<long long>(node) * ldx + f);
-                xa[2 * v] = __ldg(p);
-                xa[2 * v + 1] = __ldg(p + 1);
-            } else {
-                xa[2 * v] = xa[2 * v + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-        }
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int u = tid + 128 * v, node = nb + (u >> 6) * 8 + (u & 7), c = ((u >> 3) & 7) * 8;
-            if (node < k1) {
-                const float4* p = reinterpret_cast<const float4*>(dZ + static_cast<long long>(node) * 64 + c);
-                za[2 * v] = __ldg(p);
-                za[2 * v + 1] = __ldg(p + 1);
-            } else {
-                za[2 * v] = za[2 * v + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-        }
-        // the MMAs of stage st - 2 read this buffer: wait for their commit
-        bool ok = true;
-        if (st >= 2) ok = mbar_wait(smem_u32(mbar + b), static_cast<uint32_t>(((st - 2) >> 1) & 1), kWaitLimit);
-#pragma unroll
-        for (int v = 0; v < 8; ++v) *reinterpret_cast<uint4*>(sA + (tid + 128 * v) * 16) = pack8(xa[2 * v], xa[2 * v + 1]);
-#pragma unroll
-        for (int v = 0; v < 4; ++v) *reinterpret_cast<uint4*>(sB + (tid + 128 * v) * 16) = pack8(za[2 * v], za[2 * v + 1]);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        failed = __syncthreads_or(!ok) != 0;
-        if (failed) break;
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-#pragma unroll
-            for (int s = 0; s < S::kNodes / 16; ++s) {
-                const uint64_t da = smem_desc(a0 + s * 2 * 2048, 2048, 128);
-                const uint64_t db = smem_desc(b0 + s * 2 * 1024, 1024, 128);
-                const uint32_t accumulate = (st > 0 || s > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(mbar + b))
-                         : "memory");
-        }
-        issued = st + 1;
-    }
-    if (!failed) {
-        // the last commit completes after every MMA before it
-        const int last = stages - 1;
-        const bool ok = mbar_wait(smem_u32(mbar + (last & 1)), static_cast<uint32_t>((last >> 1) & 1), kWaitLimit);
-        failed = __syncthreads_or(!ok) != 0;
-    }
-    if (!failed) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        float* row = out + (warp * 32 + lane) * 64;
-#pragma unroll
-        for (int c0 = 0; c0 < 64; c0 += 16) {
-            uint32_t v[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-                "%14, %15}, [%16];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                *reinterpret_cast<float4*>(row + c0 + 4 * q) =
-                    make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
-                                __uint_as_float(v[4 * q + 3]));
-        }
-    } else {
-        // let the MMAs already committed finish before TMEM is freed (bounded)
-        if (tid == 0) atomicOr(err, 1u);
-        for (int b = 0; b < 2; ++b) {
-            const int st = issued - 1 - ((issued - 1 - b) & 1);   // last stage issued on buffer b
-            if (st >= 0 && (st & 1) == b) mbar_wait(smem_u32(mbar + b), static_cast<uint32_t>((st >> 1) & 1), kWaitLimit);
-        }
-        __syncthreads();
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::kCols));
-}
-
-// The weight gradient fed by cp.async: each 64-node stage of X (32 KB) and dZ (16 KB)
-// is copied as 16-byte chunks into one of ST fp32 stages (chunk c of node row k at
-// position c XOR (k mod 8); nodes past the slice are zero-filled), converted into one
-// of two bf16 MN-major buffers (the layout of k_wgrad_tc) and multiplied; ST - 1
+// one node) becomes one 16-byte core row. A 64-node bf16 buffer holds A in 16 KB (core
+// (feature block i, node block j) at j 2048 + i 128) and B in 8 KB (j 1024 + i 128);
+// with unit u = thread + 256 v, piece u lands at byte u * 16 (linear, no bank
+// conflicts): X piece u is node block u / 128, feature block (u / 8) mod 16, node u mod
+// 8; dZ piece u is node block u / 64, channel block (u / 8) mod 8, node u mod 8.
+// Each 64-node stage of X (32 KB) and dZ (16 KB) is copied by cp.async as 16-byte
+// chunks into one of ST fp32 stages (chunk c of node row k at position c XOR (k mod 8);
+// nodes past the slice are zero-filled), converted into one of two bf16 MN-major
+// buffers (the layout above) and multiplied; ST - 1
 // stages are in flight while the current one is converted. 256 threads, one CTA per
 // SM; the epilogue splits TMEM by lane quarter (warp mod 4) and column half (warp / 4).
 template <int ST>
@@ -752,7 +610,7 @@ __global__ void __launch_bounds__(256) k_wgrad_tc_pipe(int rows, int chunk, cons
         unsigned char* sA = bufs + b * S::kBuf;
         unsigned char* sB = sA + S::kABytes;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {   // X^T pieces (k_wgrad_tc numbering)
+        for (int v = 0; v < 4; ++v) {   // X^T pieces
             const int u = tid + S::kThreads * v, k = (u >> 7) * 8 + (u & 7), c = ((u >> 3) & 15) * 2;
             const unsigned char* row = xs + k * 512;
             const float4 lo = *reinterpret_cast<const float4*>(row + ((c ^ (k & 7)) << 4));
