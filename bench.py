@@ -411,7 +411,7 @@ def run_engine(args, world, rank, local):
     s = E.settings(ITERS_PER_STEP, ITERS_PER_STEP, 0.0, 0.0, 1.0, 1e-12)
 
     def step():
-        rc, x, y, r = E.pdhg(A, host, s, primal_steps=ps, dual_steps=ds, entry="preconditioned")
+        rc, x, y, r = E.pdhg(A, host, s, primal_steps=ps, dual_steps=ds, entry="preconditioned", x_out=x_out)
         if rc not in (0,):
             raise RuntimeError(f"sankhya_cuda_qp_pdhg_preconditioned returned {rc}: {E.last_error()}")
         return r
@@ -425,13 +425,15 @@ def run_engine(args, world, rank, local):
         step()
     barrier(world)
     torch.cuda.synchronize()
-    dev_ms, launches, iters = 0.0, 0, 0
+    dev_ms, launches, iters, h2d_ms, d2h_ms = 0.0, 0, 0, 0.0, 0.0
     with ClockSampler(local) as clk:
         t_start = time.perf_counter()
         for _ in range(args.steps):
             step()
             t = E.last_timing()
             dev_ms += t["loop_ms"] + t["checkpoint_ms"]
+            h2d_ms += t["h2d_ms"]
+            d2h_ms += t["d2h_ms"]
             launches += t["kernel_launches"]
             iters += t["iterations"]
         torch.cuda.synchronize()
@@ -470,7 +472,10 @@ def run_engine(args, world, rank, local):
                          "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": round(dom_ms, 4),
                          "other_launch_ms": round(d_ms if p_ms >= d_ms else p_ms, 4)},
             "e2e": {"value": round(e2e, 2), "unit": "GB/s",
-                    "h2d_bytes_per_step": 8 * (4 * n + 3 * m), "d2h_bytes_per_step": 8 * n},
+                    "h2d_bytes_per_step": 8 * (4 * n + 3 * m), "d2h_bytes_per_step": 8 * n,
+                    "wall_ms_per_step": round(1e3 * wall / max(1, args.steps), 3),
+                    "h2d_ms_per_step": round(h2d_ms / max(1, args.steps), 3),
+                    "d2h_ms_per_step": round(d2h_ms / max(1, args.steps), 3)},
             "gpu_launches": launches, "clocks": clk.summary(), "setup_s": {"generate": round(gen_s, 1),
                                                                                   "matrix_create": round(create_s, 3)}}
     if world == 1 and not args.no_time_to_kkt:

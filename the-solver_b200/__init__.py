@@ -267,15 +267,26 @@ def settings(max_iterations=1000, check_every=10, tau=0.0, sigma=0.0, theta=1.0,
     return Settings(max_iterations, check_every, tau, sigma, theta, tolerance, time_limit)
 
 
+def _out(buf, length, name):
+    """A caller's output array (float64, contiguous, `length` long), or a new one."""
+    if buf is None:
+        return np.zeros(length)
+    if buf.dtype != np.float64 or not buf.flags["C_CONTIGUOUS"] or buf.shape != (length,):
+        raise ValueError(f"{name} must be a contiguous float64 array of length {length}")
+    return buf
+
+
 def pdhg(matrix: Matrix, inst, s: Settings, hessian: Matrix | None = None, qdiag=None, primal_steps=None,
-         dual_steps=None, want_dual=False, entry: str | None = None, **over):
-    """Calls one of the five *_pdhg entry points; returns (rc, x, y, result)."""
+         dual_steps=None, want_dual=False, entry: str | None = None, x_out=None, y_out=None, **over):
+    """Calls one of the five *_pdhg entry points; returns (rc, x, y, result). x and y
+    are written into x_out / y_out when given (for example pinned host arrays, which
+    the device-to-host copies reach fastest), else into new arrays."""
     L = lib()
     get = lambda k: _d(over[k]) if k in over else _d(inst[k])
     c, rl, ru, cl, cu = get("c"), get("rl"), get("ru"), get("cl"), get("cu")
     n, m = matrix.handle.cols, matrix.handle.rows
-    x = np.zeros(n)
-    y = np.zeros(m) if want_dual else None
+    x = _out(x_out, n, "x_out")
+    y = _out(y_out, m, "y_out") if want_dual else None
     res = Result()
     qd, ps, ds = _d(qdiag), _d(primal_steps), _d(dual_steps)
     h = C.byref(hessian.handle) if hessian is not None else None
