@@ -327,7 +327,8 @@ def _pdlp_run(E, A, inst, eps, precision, algorithm, limit_s, oracle):
 def time_to_kkt(E, A, inst, eps_list=(1e-4, 1e-6, 1e-8), limit_s=120.0, halpern=False, limit_1e8_s=60.0):
     """Wall time of sankhya_b200_pdlp_solve to each relative-KKT tolerance on the same
     instance: plain FP64 PDLP (GpuPdlp's restarted adaptive loop) versus FP32 inner
-    iterations refined in FP64 at every restart. Host arrays in and out, scaling
+    iterations refined in FP64 at every restart, with FP32 and with bf16 matrix values
+    (FP32 products). Host arrays in and out, scaling
     included. Each run's objective is compared with the FP64 oracle value of the
     instance (the tightest FP64 solves of two independent codes) where it is present.
     With halpern, the reflected restarted Halpern loop runs at the middle tolerance.
@@ -340,7 +341,8 @@ def time_to_kkt(E, A, inst, eps_list=(1e-4, 1e-6, 1e-8), limit_s=120.0, halpern=
         key = f"eps_{eps:.0e}"
         lim = limit_1e8_s if eps < 1e-7 else limit_s
         row = {"fp64": _pdlp_run(E, A, inst, eps, E.FP64, E.PDLP_ADAPTIVE, lim, oracle),
-               "fp32_refined": _pdlp_run(E, A, inst, eps, E.FP32_REFINE, E.PDLP_ADAPTIVE, lim, oracle)}
+               "fp32_refined": _pdlp_run(E, A, inst, eps, E.FP32_REFINE, E.PDLP_ADAPTIVE, lim, oracle),
+               "bf16_values_refined": _pdlp_run(E, A, inst, eps, E.BF16_REFINE, E.PDLP_ADAPTIVE, lim, oracle)}
         if halpern and eps == eps_list[len(eps_list) // 2]:
             row["halpern_fp64"] = _pdlp_run(E, A, inst, eps, E.FP64, E.PDLP_HALPERN, limit_s, oracle)
         for name in [k for k in row if k != "fp64"]:

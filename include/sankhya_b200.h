@@ -135,7 +135,7 @@ enum {
 
 enum {
     SANKHYA_B200_FP64 = 0,       /* FP64 everywhere                                  */
-    SANKHYA_B200_FP32_REFINE = 1 /* FP32 inner iterations, FP64 refinement residuals:
+    SANKHYA_B200_FP32_REFINE = 1, /* FP32 inner iterations, FP64 refinement residuals:
                                     with the adaptive step, the iterations run in FP32 on
                                     deviations from an FP64 center that moves to the
                                     restart point at every restart (one refinement: the
@@ -144,6 +144,10 @@ enum {
                                     use FP64 residuals of center + deviation. With the
                                     Halpern loop or the fixed step: an FP32 phase to
                                     1e-4, then an FP64 finish.                         */
+    SANKHYA_B200_BF16_REFINE = 2 /* as FP32_REFINE (adaptive loop only), with the
+                                    scaled matrix values of the FP32 iterations rounded
+                                    to bf16 (products accumulate in FP32); the center's
+                                    products and all residuals use the FP64 values.    */
 };
 
 enum {
@@ -161,7 +165,7 @@ typedef struct SankhyaB200PdlpSettings {
     int adaptive_step;    /* 1: Applegate et al. adaptive step; 0: 0.9/||A||_2    */
     int scaling;          /* bitmask of SANKHYA_B200_SCALE_*                      */
     int ruiz_iterations;  /* 100                                                  */
-    int precision;        /* SANKHYA_B200_FP64 or SANKHYA_B200_FP32_REFINE        */
+    int precision;        /* SANKHYA_B200_FP64, _FP32_REFINE or _BF16_REFINE      */
     double eps_optimal;   /* relative KKT tolerance on all three measures         */
     double time_limit;    /* seconds, <= 0 for none                               */
     double eta_min_factor;/* 1e-6 */

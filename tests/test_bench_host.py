@@ -25,7 +25,7 @@ class _Settings:
 
 class _FakeEngine:
     """pdlp_solve answers from a table keyed by (precision, algorithm)."""
-    FP64, FP32_REFINE, PDLP_ADAPTIVE, PDLP_HALPERN = 0, 1, 0, 1
+    FP64, FP32_REFINE, BF16_REFINE, PDLP_ADAPTIVE, PDLP_HALPERN = 0, 1, 2, 0, 1
 
     def __init__(self, answers):
         self.answers = answers
@@ -51,12 +51,12 @@ def test_iteration_bytes_are_the_two_launches():
 
 
 def test_time_to_kkt_reports_speedups_and_objective_error(monkeypatch):
-    """One row per tolerance: FP64 and FP32-refined runs, the speed-up where both
+    """One row per tolerance: FP64, FP32-refined and bf16-value runs, the speed-up where both
     converged, and each objective's relative error against the oracle value."""
     b = _bench()
     monkeypatch.setattr(b, "oracle_objective", lambda: -1.0)
     inst = {"c": np.array([1.0, -2.0])}
-    E = _FakeEngine({(0, 0): (0, [1.0, 1.0]), (1, 0): (0, [1.0, 1.0 + 1e-7]),
+    E = _FakeEngine({(0, 0): (0, [1.0, 1.0]), (1, 0): (0, [1.0, 1.0 + 1e-7]), (2, 0): (0, [1.0, 1.0 + 2e-7]),
                      (0, 1): (1, [0.0, 0.0]), (1, 1): (0, [np.nan, 0.0])})
     out = b.time_to_kkt(E, None, inst, eps_list=(1e-4, 1e-6, 1e-8), halpern=True)
     assert out["oracle_objective"] == -1.0
@@ -66,6 +66,8 @@ def test_time_to_kkt_reports_speedups_and_objective_error(monkeypatch):
         assert abs(row["fp32_refined"]["objective_rel_err_vs_oracle"] - 2e-7 / 2.0) < 1e-15
         assert row["fp32_refined"]["refinements"] == 4
         assert "speedup_fp32_refined_vs_fp64" in row
+        assert abs(row["bf16_values_refined"]["objective_rel_err_vs_oracle"] - 4e-7 / 2.0) < 1e-15
+        assert "speedup_bf16_values_refined_vs_fp64" in row
     assert "halpern_fp64" in out["eps_1e-06"] and "halpern_fp64" not in out["eps_1e-04"]
     assert "speedup_halpern_fp64_vs_fp64" not in out["eps_1e-06"]     # that run did not converge
     assert out["eps_1e-06"]["halpern_fp64"]["objective_rel_err_vs_oracle"] == 0.5
@@ -76,7 +78,7 @@ def test_time_to_kkt_without_oracle_and_nan_objective(monkeypatch):
     """No oracle file: no error entries; a NaN objective is reported as null (strict JSON)."""
     b = _bench()
     monkeypatch.setattr(b, "oracle_objective", lambda: None)
-    E = _FakeEngine({(0, 0): (0, [1.0]), (1, 0): (0, [np.nan])})
+    E = _FakeEngine({(0, 0): (0, [1.0]), (1, 0): (0, [np.nan]), (2, 0): (0, [1.0])})
     out = b.time_to_kkt(E, None, {"c": np.array([1.0])}, eps_list=(1e-6,))
     row = out["eps_1e-06"]
     assert "objective_rel_err_vs_oracle" not in row["fp64"]

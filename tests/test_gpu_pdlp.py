@@ -123,11 +123,12 @@ def test_fp32_refined_reaches_simplex_objective(engine, instances, golden_dir, n
     assert abs(obj - ref["objective"]) <= 1e-6 * (1 + abs(ref["objective"])), (obj, ref)
 
 
-@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE"])
+@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE", "BF16_REFINE"])
 def test_config0_to_1e8_reaches_the_simplex_objective(engine, instances, golden_dir, precision):
-    """The 2,000 x 5,000 LP (instances.lp_config0, seed 0) to 1e-8 relative KKT, FP64
-    and FP32 iterations refined in FP64: the objective matches the reference simplex's
-    (certified by its sk_verify, cross-checked with HiGHS) to 1e-6 relative."""
+    """The 2,000 x 5,000 LP (instances.lp_config0, seed 0) to 1e-8 relative KKT, FP64,
+    FP32 iterations refined in FP64, and FP32 iterations over bf16 matrix values refined
+    in FP64: the objective matches the reference simplex's (certified by its sk_verify,
+    cross-checked with HiGHS) to 1e-6 relative."""
     g = json.load(open(os.path.join(golden_dir, "simplex_lp_config0.json")))
     inst = instances.lp_config0(0)
     A = engine.Matrix.from_instance(inst)
@@ -139,7 +140,8 @@ def test_config0_to_1e8_reaches_the_simplex_objective(engine, instances, golden_
     assert abs(obj - g["objective"]) <= 1e-6 * (1 + abs(g["objective"])), (obj, g["objective"])
 
 
-def test_fp32_refined_agrees_with_fp64_on_power_law(engine, instances):
+@pytest.mark.parametrize("precision", ["FP32_REFINE", "BF16_REFINE"])
+def test_refined_agrees_with_fp64_on_power_law(engine, instances, precision):
     """|a| over six decades. The restarted loop's progress past ~1e-5 on such matrices
     depends on the exact rounding of its trajectory (FP64 runs of two implementations
     stall at different gaps), so the check is at 1e-5, where both converge. A relative
@@ -148,8 +150,8 @@ def test_fp32_refined_agrees_with_fp64_on_power_law(engine, instances):
     inst = instances.lp_powerlaw(21, 4000, 8000, 80000)
     A = engine.Matrix.from_instance(inst)
     rc64, x64, y64, r64 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-5, time_limit=60.0))
-    rc32, x32, y32, r32 = engine.pdlp_solve(A, inst, settings(engine, precision=engine.FP32_REFINE, eps_optimal=1e-5,
-                                                              time_limit=60.0))
+    rc32, x32, y32, r32 = engine.pdlp_solve(A, inst, settings(engine, precision=getattr(engine, precision),
+                                                              eps_optimal=1e-5, time_limit=60.0))
     assert rc64 == 0 and rc32 == 0 and r64["status"] == 0 and r32["status"] == 0, (r64, r32)
     o64, o32 = float(np.dot(inst["c"], x64)), float(np.dot(inst["c"], x32))
     assert abs(o64 - o32) <= 1e-4 * (1 + abs(o64))
@@ -173,6 +175,28 @@ def test_fp32_centered_loop_follows_fp64(engine, instances, eps):
     assert max(r32["relative_primal_residual"], r32["relative_dual_residual"], r32["relative_gap"]) <= eps
     o64, o32 = float(np.dot(inst["c"], x64)), float(np.dot(inst["c"], x32))
     assert abs(o64 - o32) <= 10 * eps * (1 + abs(o64)), (o64, o32)
+
+
+def test_bf16_values_centered_loop(engine, instances):
+    """bf16 matrix values under the FP32 deviations: the residuals and restart decisions
+    stay in FP64 on the exact matrix, so the solve still reaches the FP64 tolerance
+    and objective, in a number of iterations near the FP64 solve's (printed with -s);
+    the mode needs the adaptive loop."""
+    inst = instances.lp_uniform(3, 5000, 10000, 5)
+    A = engine.Matrix.from_instance(inst)
+    rc64, x64, _, r64 = engine.pdlp_solve(A, inst, settings(engine, eps_optimal=1e-6, time_limit=60.0))
+    rc16, x16, _, r16 = engine.pdlp_solve(A, inst, settings(engine, precision=engine.BF16_REFINE, eps_optimal=1e-6,
+                                                            time_limit=60.0))
+    assert rc64 == rc16 == 0 and r64["status"] == r16["status"] == 0, (r64, r16)
+    assert r16["refinements"] > 1
+    assert r16["iterations"] <= 2 * r64["iterations"] + 256, (r16["iterations"], r64["iterations"])
+    assert max(r16["relative_primal_residual"], r16["relative_dual_residual"], r16["relative_gap"]) <= 1e-6
+    o64, o16 = float(np.dot(inst["c"], x64)), float(np.dot(inst["c"], x16))
+    assert abs(o64 - o16) <= 1e-5 * (1 + abs(o64)), (o64, o16)
+    print(f"\nBF16_REFINE {r16['iterations']} it {r16['seconds']:.3f} s vs FP64 {r64['iterations']} it "
+          f"{r64['seconds']:.3f} s")
+    rc, *_ = engine.pdlp_solve(A, inst, settings(engine, precision=engine.BF16_REFINE, algorithm=engine.PDLP_HALPERN))
+    assert rc == -1 and "BF16_REFINE" in engine.last_error()
 
 
 # ------------------------------------------------------- reflected Halpern PDHG option

@@ -153,7 +153,7 @@ class GnnSettings(C.Structure):
 
 
 SCALE_RUIZ, SCALE_POCK_CHAMBOLLE, SCALE_POW2 = 1, 2, 4
-FP64, FP32_REFINE = 0, 1
+FP64, FP32_REFINE, BF16_REFINE = 0, 1, 2
 PDLP_ADAPTIVE, PDLP_HALPERN = 0, 1
 
 

@@ -10,6 +10,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 
 #include <cmath>
 #include <cstdint>
@@ -265,8 +266,19 @@ __device__ __forceinline__ void prefetch_l2(const T* base, int first, int last) 
                      : "memory");
 }
 
-template <class Epi, class T>
-__global__ void __launch_bounds__(kThreads) k_tiled(TileCsrT<T> A, const T* __restrict__ v, Epi epi) {
+// A stored matrix value as the arithmetic type T (the identity unless the values
+// are kept narrower than the vectors, e.g. bf16 values with fp32 vectors).
+template <class T, class V>
+__device__ __forceinline__ T load_value(const V* p) {
+    return static_cast<T>(__ldcs(p));
+}
+template <>
+__device__ __forceinline__ float load_value<float, __nv_bfloat16>(const __nv_bfloat16* p) {
+    return __bfloat162float(__ldcs(p));
+}
+
+template <class Epi, class T, class V = T>
+__global__ void __launch_bounds__(kThreads) k_tiled(TileCsrT<V> A, const T* __restrict__ v, Epi epi) {
     using P = RowPre<Epi>;
     __shared__ T prod[kWarps][kChunkNnz];
     __shared__ double red[kWarps * 8];
@@ -304,10 +316,10 @@ __global__ void __launch_bounds__(kThreads) k_tiled(TileCsrT<T> A, const T* __re
             T s0 = T(0), s1 = T(0);
             int p = p0 + lane;
             for (; p + 32 < p1; p += 64) {
-                s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
-                s1 += __ldcs(A.val + p + 32) * __ldg(v + __ldcs(A.idx + p + 32));
+                s0 += load_value<T>(A.val + p) * __ldg(v + __ldcs(A.idx + p));
+                s1 += load_value<T>(A.val + p + 32) * __ldg(v + __ldcs(A.idx + p + 32));
             }
-            if (p < p1) s0 += __ldcs(A.val + p) * __ldg(v + __ldcs(A.idx + p));
+            if (p < p1) s0 += load_value<T>(A.val + p) * __ldg(v + __ldcs(A.idx + p));
             const T s = warp_sum(s0 + s1);
             if (lane == 0) P::apply(epi, r0, s, pre, acc);
             b0 = n0;
@@ -323,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) k_tiled(TileCsrT<T> A, const T* __re
             a[k] = T(0);
             if (p < p1) {
                 col[k] = __ldcs(A.idx + p);
-                a[k] = __ldcs(A.val + p);
+                a[k] = load_value<T>(A.val + p);
             }
         }
 #pragma unroll
@@ -366,16 +378,16 @@ struct StoreEpiT {
 };
 using StoreEpi = StoreEpiT<double>;
 
-template <class Epi, class T = double>
-inline int tiled_grid(const TileCsrT<T>& A) {
-    const void* k = reinterpret_cast<const void*>(&k_tiled<Epi, T>);
+template <class Epi, class T = double, class V = T>
+inline int tiled_grid(const TileCsrT<V>& A) {
+    const void* k = reinterpret_cast<const void*>(&k_tiled<Epi, T, V>);
     return grid_for(k, (A.ntiles + kWarps - 1) / kWarps, 0);
 }
 
-template <class Epi, class T>
-inline int launch_tiled(const TileCsrT<T>& A, const T* v, const Epi& epi, cudaStream_t stream, int grid) {
+template <class Epi, class T, class V>
+inline int launch_tiled(const TileCsrT<V>& A, const T* v, const Epi& epi, cudaStream_t stream, int grid) {
     if (A.ntiles == 0) return 0;
-    k_tiled<Epi, T><<<grid, kThreads, 0, stream>>>(A, v, epi);
+    k_tiled<Epi, T, V><<<grid, kThreads, 0, stream>>>(A, v, epi);
     return 0;
 }
 

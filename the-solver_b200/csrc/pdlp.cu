@@ -942,6 +942,14 @@ __global__ void k_narrow(long long n, const double* __restrict__ in, float* __re
         out[j] = static_cast<float>(in[j]);
 }
 
+// The scaled matrix values rounded to bf16 (round to nearest even) for the
+// BF16_REFINE iterations.
+__global__ void k_narrow_bf16(long long n, const double* __restrict__ in, __nv_bfloat16* __restrict__ out) {
+    for (long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; j < n;
+         j += static_cast<long long>(blockDim.x) * gridDim.x)
+        out[j] = __double2bfloat16(in[j]);
+}
+
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -1146,13 +1154,14 @@ struct LoopStats {
     Kkt best;
 };
 
-// Restarted PDLP on one problem whose data (c, bounds) and matrix views have
-// value type T; iterates of type T; reductions and decisions in FP64.
-template <class T>
+// Restarted PDLP on one problem whose data (c, bounds) have type T and whose matrix
+// values have type V (T, or bf16 under fp32 iterates); iterates of type T; reductions
+// and decisions in FP64.
+template <class T, class V = T>
 struct Core {
     int n = 0, m = 0, sms = 148;
     cudaStream_t stream = nullptr;
-    TileCsrT<T> A, AT;
+    TileCsrT<V> A, AT;
     const T *c = nullptr, *cl = nullptr, *cu = nullptr, *rl = nullptr, *ru = nullptr;
     DevBuf blob;
     T *x, *x_cand, *x_sum, *x_avg, *x_restart, *x_bar, *aty;
@@ -1215,7 +1224,7 @@ struct Core {
         return 0;
     }
 
-    void set_problem(const TileCsrT<T>& a, const TileCsrT<T>& at, const T* c_, const T* cl_, const T* cu_,
+    void set_problem(const TileCsrT<V>& a, const TileCsrT<V>& at, const T* c_, const T* cl_, const T* cu_,
                      const T* rl_, const T* ru_) {
         A = a;
         AT = at;
@@ -1722,7 +1731,9 @@ int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, cons
         return fail_msg("null model or output pointer");
     if (s.max_iterations <= 0 || s.restart_period <= 0 || s.power_iterations < 0 || !(s.eps_optimal > 0.0) ||
         s.time_limit < 0.0 || !(s.eta_min_factor > 0.0) || !(s.eta_max_factor >= s.eta_min_factor) ||
-        s.ruiz_iterations < 0 || (s.precision != SANKHYA_B200_FP64 && s.precision != SANKHYA_B200_FP32_REFINE))
+        s.ruiz_iterations < 0 ||
+        (s.precision != SANKHYA_B200_FP64 && s.precision != SANKHYA_B200_FP32_REFINE &&
+         s.precision != SANKHYA_B200_BF16_REFINE))
         return fail_msg("invalid PDLP settings");
     const int n = matrix->cols, m = matrix->rows;
     const bool quadratic = hessian != nullptr || qdiag != nullptr;
@@ -1733,6 +1744,8 @@ int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, cons
             if (!std::isfinite(qdiag[j]) || qdiag[j] < 0.0) return fail_msg("invalid quadratic diagonal");
     if (quadratic && (s.algorithm != SANKHYA_B200_PDLP_ADAPTIVE || !s.adaptive_step))
         return fail_msg("the QP solve runs the adaptive step of the restarted loop");
+    if (s.precision == SANKHYA_B200_BF16_REFINE && (s.algorithm != SANKHYA_B200_PDLP_ADAPTIVE || !s.adaptive_step))
+        return fail_msg("BF16_REFINE runs the adaptive step of the restarted loop");
     for (int j = 0; j < n; ++j)
         if (!std::isfinite(c[j]) || std::isnan(col_lower[j]) || std::isnan(col_upper[j]) || col_lower[j] > col_upper[j])
             return fail_msg("invalid cost or column bound");
@@ -1835,13 +1848,28 @@ int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, cons
         launches += hi.launches;
     } else if (lp.adaptive && !lp.halpern) {
         // ------------------------- FP32 iterations around an FP64 center, refined at restarts
+        // (matrix values in FP32, or in bf16 for BF16_REFINE; the center's products and
+        // every residual use the FP64 values)
         DevBuf vals32, blob32, cbuf;
         const size_t nnz = static_cast<size_t>(plan->a.nnz);
-        if (vals32.alloc(nnz * 8 + 1024, "cudaMalloc FP32 values")) return -1;
-        float* a32 = vals32.as<float>();
-        float* at32 = a32 + (nnz + 63) / 64 * 64;
-        k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.A.val, a32);
-        k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.AT.val, at32);
+        const bool bf16 = s.precision == SANKHYA_B200_BF16_REFINE;
+        const size_t vbytes = bf16 ? 2 : 4;
+        if (vals32.alloc(nnz * 2 * vbytes + 1024, "cudaMalloc narrowed values")) return -1;
+        float* a32 = nullptr;
+        float* at32 = nullptr;
+        __nv_bfloat16* a16 = nullptr;
+        __nv_bfloat16* at16 = nullptr;
+        if (bf16) {
+            a16 = vals32.as<__nv_bfloat16>();
+            at16 = a16 + (nnz + 127) / 128 * 128;
+            k_narrow_bf16<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.A.val, a16);
+            k_narrow_bf16<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.AT.val, at16);
+        } else {
+            a32 = vals32.as<float>();
+            at32 = a32 + (nnz + 63) / 64 * 64;
+            k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.A.val, a32);
+            k_narrow<<<sc.sms * 8, kThreads, 0, stream>>>(static_cast<long long>(nnz), sc.AT.val, at32);
+        }
         const size_t nf = (static_cast<size_t>(n) * 4 + 255) / 256 * 256;
         const size_t mf = (static_cast<size_t>(m) * 4 + 255) / 256 * 256;
         const size_t nd = (static_cast<size_t>(n) * 8 + 255) / 256 * 256;
@@ -1888,21 +1916,29 @@ int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, cons
             qd32 = q32buf.as<float>();
             k_narrow<<<eg(n), kThreads, 0, stream>>>(n, qd_s, qd32);
         }
-        Core<float> lo;
-        lo.stream = stream;
-        lo.host = hs.p;
-        if (lo.allocate(n, m, sc.sms)) return -1;
-        if (lo.set_hessian(qd32, hessian ? &Q32 : nullptr)) return -1;
-        lo.set_problem(sc.A.with_values<float>(a32), sc.AT.with_values<float>(at32), ctr.c32, ctr.cl32, ctr.cu32,
-                       ctr.rl32, ctr.ru32);
-        lo.ctr = &ctr;
         lp.eps = s.eps_optimal;
         lp.max_iterations = s.max_iterations;
         lp.cost_norm = cost_norm;
         lp.bound_norm = bound_norm;
-        if (lo.run(lp, &stats)) return -1;
-        refinements = lo.recenters;
-        launches += hi.launches + lo.launches;
+        auto run_lo = [&](auto& lo, const auto& av, const auto& atv) -> int {
+            lo.stream = stream;
+            lo.host = hs.p;
+            if (lo.allocate(n, m, sc.sms)) return -1;
+            if (lo.set_hessian(qd32, hessian ? &Q32 : nullptr)) return -1;
+            lo.set_problem(av, atv, ctr.c32, ctr.cl32, ctr.cu32, ctr.rl32, ctr.ru32);
+            lo.ctr = &ctr;
+            if (lo.run(lp, &stats)) return -1;
+            refinements = lo.recenters;
+            launches += hi.launches + lo.launches;
+            return 0;
+        };
+        if (bf16) {
+            Core<float, __nv_bfloat16> lo;
+            if (run_lo(lo, sc.A.with_values<__nv_bfloat16>(a16), sc.AT.with_values<__nv_bfloat16>(at16))) return -1;
+        } else {
+            Core<float> lo;
+            if (run_lo(lo, sc.A.with_values<float>(a32), sc.AT.with_values<float>(at32))) return -1;
+        }
     } else {
         // ------------- Halpern or fixed-step loop: FP32 iterations, then an FP64 finish
         DevBuf vals32, blob32;
