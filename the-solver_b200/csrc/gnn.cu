@@ -616,7 +616,7 @@ template <int N, int K>
 void gemm_tc(SankhyaB200Gnn* s, cudaStream_t st, int M, const float* A, int lda, const __nv_bfloat16* B, int sbk,
              int sbn, const float* bias, int relu, float* C, int ldc) {
     if constexpr (K == 128) {
-        gemm_tc_pipe<N, K, 2>(s, st, M, A, lda, B, sbk, sbn, bias, relu, C, ldc);
+        gemm_tc_pipe<N, K, 4>(s, st, M, A, lda, B, sbk, sbn, bias, relu, C, ldc);
         return;
     } else if constexpr (K == 64) {
         gemm_tc_pipe<N, K, 3>(s, st, M, A, lda, B, sbk, sbn, bias, relu, C, ldc);

@@ -303,9 +303,10 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, const float* __restrict_
 // ------------------------------------------------------ layer GEMM, pipelined
 //
 // The same product for K in {64, 128}, fed by cp.async instead of register-staged
-// loads, so that a CTA keeps ST - 1 fp32 tiles (64 or 32 KB each) in flight while it
-// converts, multiplies and writes back the current one:
-//   - a tile's 16-byte chunks (row r, chunk c) are copied to row r of an fp32 stage
+// loads. A stage is a 64-column K-slice of a tile (32 KB of fp32), so that a CTA keeps
+// ST - 1 slices (1.5 to 2 tiles) in flight while it converts, multiplies and writes
+// back the current tile:
+//   - a slice's 16-byte chunks (row r, chunk c) are copied to row r of an fp32 stage
 //     at chunk position c XOR (r mod 8) (rows past M are zero-filled by a source size
 //     of 0 and read nothing);
 //   - the threads convert the stage to bf16 in the canonical K-major layout, piece u
@@ -331,8 +332,10 @@ struct TcPipeShape {
     static_assert(ST >= 2 && ST <= 4, "2 to 4 stages");
     static constexpr int kThreads = 256;
     static constexpr int kM = 128;
-    static constexpr int kChunks = K / 4;                 // 16-byte chunks per fp32 row
-    static constexpr int kStageBytes = kM * K * 4;        // one fp32 tile
+    static constexpr int kKS = 64;                        // k columns per stage (a K-slice)
+    static constexpr int kSlices = K / kKS;               // stages per tile
+    static constexpr int kChunks = kKS / 4;               // 16-byte chunks per fp32 slice row
+    static constexpr int kStageBytes = kM * kKS * 4;      // one fp32 K-slice of a tile
     static constexpr int kABytes = kM * K * 2;            // bf16 canonical A
     static constexpr int kBBytes = N * K * 2;             // bf16 canonical B
     static constexpr int kEpiBytes = 8 * 32 * 16 * 4;     // 8 warps x 32 rows x 16 floats
@@ -341,7 +344,7 @@ struct TcPipeShape {
 };
 
 template <int N, int K, int ST>
-__global__ void __launch_bounds__(256) k_gemm_tc_pipe(int M, const float* __restrict__ A, int lda,
+__global__ void __launch_bounds__(256, 1) k_gemm_tc_pipe(int M, const float* __restrict__ A, int lda,
                                                       const __nv_bfloat16* __restrict__ B, int sbk, int sbn,
                                                       const float* __restrict__ bias, int relu, float* __restrict__ C,
                                                       int ldc, unsigned int* __restrict__ err) {
@@ -357,25 +360,26 @@ __global__ void __launch_bounds__(256) k_gemm_tc_pipe(int M, const float* __rest
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles = (M + S::kM - 1) / S::kM;
 
-    // fp32 tile `tile` into stage `s` (an empty group past the last tile keeps the
-    // group count uniform)
-    auto issue = [&](int tile, int s) {
+    // Unit j of this CTA is K-slice j mod kSlices of its tile j / kSlices; it goes to
+    // stage j mod ST (an empty group past the last tile keeps the group count uniform).
+    const int t0 = blockIdx.x;
+    auto issue = [&](int j) {
+        const int tile = t0 + (j / S::kSlices) * gridDim.x, k0 = (j % S::kSlices) * S::kKS;
         if (tile < tiles) {
             const int m0 = tile * S::kM;
-            const uint32_t base = smem_u32(stages + s * S::kStageBytes);
+            const uint32_t base = smem_u32(stages + (j % ST) * S::kStageBytes);
 #pragma unroll 4
             for (int q = tid; q < S::kM * S::kChunks; q += S::kThreads) {
                 const int r = q / S::kChunks, c = q - r * S::kChunks;
                 const bool live = m0 + r < M;
-                const float* src = A + static_cast<long long>(live ? m0 + r : 0) * lda + c * 4;
-                cp_async16(base + r * (K * 4) + ((c ^ (r & 7)) << 4), src, live ? 16 : 0);
+                const float* src = A + static_cast<long long>(live ? m0 + r : 0) * lda + k0 + c * 4;
+                cp_async16(base + r * (S::kKS * 4) + ((c ^ (r & 7)) << 4), src, live ? 16 : 0);
             }
         }
         cp_async_commit();
     };
-    const int t0 = blockIdx.x;
 #pragma unroll
-    for (int s = 0; s < ST - 1; ++s) issue(t0 + s * gridDim.x, s);
+    for (int j = 0; j < ST - 1; ++j) issue(j);
 
     // B pieces as in k_gemm_tc
 #pragma unroll 4
@@ -417,21 +421,29 @@ __global__ void __launch_bounds__(256) k_gemm_tc_pipe(int M, const float* __rest
     float* stg = sE + warp * 32 * 16;
     int i = 0;
     for (int tile = t0; tile < tiles; tile += gridDim.x, ++i) {
-        const int m0 = tile * S::kM, s = i % ST;
-        // the stage converted in the previous iteration takes tile i + ST - 1
-        issue(tile + (ST - 1) * gridDim.x, (i + ST - 1) % ST);
-        cp_async_wait<ST - 1>();
-        __syncthreads();
-        const unsigned char* st = stages + s * S::kStageBytes;
+        const int m0 = tile * S::kM;
 #pragma unroll
-        for (int v = 0; v < K / 16; ++v) {
-            const int u = tid + S::kThreads * v;
-            int r, k;
-            unit_row_k<K>(u, r, k);
-            const unsigned char* row = st + r * (K * 4);
-            const float4 lo = *reinterpret_cast<const float4*>(row + (((k >> 2) ^ (r & 7)) << 4));
-            const float4 hi = *reinterpret_cast<const float4*>(row + ((((k >> 2) + 1) ^ (r & 7)) << 4));
-            *reinterpret_cast<uint4*>(sA + u * 16) = pack8(lo, hi);
+        for (int sl = 0; sl < S::kSlices; ++sl) {
+            const int j = i * S::kSlices + sl;
+            // the stage converted last takes unit j + ST - 1
+            issue(j + ST - 1);
+            cp_async_wait<ST - 1>();
+            __syncthreads();
+            const unsigned char* st = stages + (j % ST) * S::kStageBytes;
+            // slice pieces (8 k of one row) numbered as in unit_row_k over the slice's
+            // kKS columns; piece (r, k) of the tile lands at kmajor_offset<K>(r, k)
+#pragma unroll
+            for (int v = 0; v < S::kKS / 16; ++v) {
+                const int u = tid + S::kThreads * v;
+                int r, k;
+                unit_row_k<S::kKS>(u, r, k);
+                const unsigned char* row = st + r * (S::kKS * 4);
+                const float4 lo = *reinterpret_cast<const float4*>(row + (((k >> 2) ^ (r & 7)) << 4));
+                const float4 hi = *reinterpret_cast<const float4*>(row + ((((k >> 2) + 1) ^ (r & 7)) << 4));
+                *reinterpret_cast<uint4*>(sA + kmajor_offset<K>(r, sl * S::kKS + k)) = pack8(lo, hi);
+            }
+            // the next slice's issue reuses the stage just read
+            if (sl + 1 < S::kSlices) __syncthreads();
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
