@@ -45,6 +45,7 @@ def load(name: str) -> C.CDLL:
                 "ref_scaling": os.path.join(HERE, "_ref", "libsihps_scaling_ref.so"),
                 "ref_pdlp": os.path.join(HERE, "_ref", "libsihps_pdlp_ref.so"),
                 "ref_hooked": os.path.join(HERE, "_ref", "libsankhya_ref_hooked.so"),
+                "ref_milp_hooked": os.path.join(HERE, "_ref", "libsankhya_ref_milp_hooked.so"),
                 "ref_lp": os.path.join(HERE, "_ref", "libsihps_lp_ref.so"),
                 "ref_lp_hooked": os.path.join(HERE, "_ref", "libsihps_lp_hooked.so"),
                 "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so")}[name]
