@@ -52,5 +52,5 @@ def test_search_through_the_engine_matches_the_reference_search(engine, hooked, 
     assert abs(r1["objective"] - r0["objective"]) <= 1e-9 * (1 + abs(r0["objective"]))
     assert r1["iterations"] < r0["iterations"] / 10, (r1["iterations"], r0["iterations"])
     assert t["iterations"] > 0 and t["checkpoints"] > 0, t
-    print(f"\\n32 binaries: {r1['nodes']} nodes through the engine, {r1['iterations']} simplex pivots "
+    print(f"\n32 binaries: {r1['nodes']} nodes through the engine, {r1['iterations']} simplex pivots "
           f"(reference: {r0['nodes']} nodes, {r0['iterations']} pivots)")
