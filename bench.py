@@ -352,6 +352,53 @@ def time_to_kkt(E, A, inst, eps_list=(1e-4, 1e-6, 1e-8), limit_s=120.0, halpern=
     return out
 
 
+def config0_to_1e8(E, I, reps=3):
+    """Config 0 (2,000 x 5,000, the metric's 1e-8 tolerance): wall time of
+    sankhya_b200_pdlp_solve to 1e-8 relative KKT, host arrays in and out, for FP64 and
+    the two refined modes (best of `reps` after an untimed solve), each objective
+    against the reference simplex's (tests/golden/simplex_lp_config0.json, certified
+    by its sk_verify); and the reference's own GPU PDLP to the same tolerance on the
+    same GPU, as in reference_gpu."""
+    inst = I.lp_config0(0)
+    golden = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "simplex_lp_config0.json")) as f:
+            golden = float(json.load(f)["objective"])
+    except (OSError, KeyError, ValueError):
+        pass
+    A = E.Matrix.from_instance(inst)
+    out = {"workload": "lp_config0: m=2000, n=5000, 5 per column, seed 0", "eps": 1e-8,
+           "oracle": "tests/golden/simplex_lp_config0.json (the reference's simplex)", "oracle_objective": golden}
+    for name, prec in (("fp64", E.FP64), ("fp32_refined", E.FP32_REFINE), ("bf16_values_refined", E.BF16_REFINE)):
+        _pdlp_run(E, A, inst, 1e-8, prec, E.PDLP_ADAPTIVE, 60.0, golden)
+        runs = [_pdlp_run(E, A, inst, 1e-8, prec, E.PDLP_ADAPTIVE, 60.0, golden) for _ in range(reps)]
+        out[name] = min(runs, key=lambda r: r["seconds"])
+    A.close()
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.ref_gpupdlp(inst, eps=1e-8, time_limit=60.0, scale=True)
+        best = None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            x, st = O.ref_gpupdlp(inst, eps=1e-8, time_limit=60.0, scale=True)
+            wall = time.perf_counter() - t0
+            if best is None or wall < best[0]:
+                best = (wall, x, st)
+        wall, x, st = best
+        obj = _finite(np.dot(inst["c"], x))
+        g = {"seconds": round(wall, 3), "converged": st["converged"], "iterations": st["iterations"],
+             "objective": obj}
+        if golden is not None and obj is not None:
+            g["objective_rel_err_vs_oracle"] = _finite(abs(obj - golden) / (1.0 + abs(golden)))
+        out["reference_gpupdlp"] = g
+        if st["converged"] == 1 and out["fp64"]["status"] == 0:
+            out["engine_fp64_speedup_vs_reference_gpupdlp"] = round(wall / out["fp64"]["seconds"], 2)
+    except (OSError, FileNotFoundError, RuntimeError) as exc:
+        out["reference_gpupdlp"] = {"unavailable": str(exc)}
+    return out
+
+
 def _finite(v):
     """A float for the JSON line, or None where it is not finite (NaN is not JSON)."""
     v = float(v)
@@ -482,6 +529,7 @@ def run_engine(args, world, rank, local):
                                                                                   "matrix_create": round(create_s, 3)}}
     if world == 1 and not args.no_time_to_kkt:
         line["time_to_kkt"] = time_to_kkt(E, A, inst)
+        line["config0_time_to_1e8"] = config0_to_1e8(E, I)
     if world == 1 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_baseline(E, A, inst, ps, ds)
         ttk = line.get("time_to_kkt", {}).get("eps_1e-06", {}).get("fp64", {})

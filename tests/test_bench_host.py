@@ -153,3 +153,46 @@ def test_committed_traffic_figures_parse_as_the_bench_reads_them():
     for key in ("primal", "dual"):
         v = int(figures[key])
         assert 1e8 < v < 1e9, (key, v)
+
+
+def test_config0_leg_reports_each_mode_against_the_simplex(monkeypatch):
+    """The config-0 leg: one row per precision with its objective error against the
+    simplex golden, the best of the timed solves, and a reference row (here
+    unavailable, as on a machine without the reference build)."""
+    b = _bench()
+    calls = []
+
+    class _I:
+        @staticmethod
+        def lp_config0(seed):
+            return {"c": np.array([1.0, -2.0]), "m": 1, "n": 2}
+
+    class _E(_FakeEngine):
+        class Matrix:
+            @staticmethod
+            def from_instance(inst):
+                class _M:
+                    def close(self):
+                        calls.append("close")
+                return _M()
+
+    E = _E({(0, 0): (0, [1.0, 1.0]), (1, 0): (0, [1.0, 1.0]), (2, 0): (0, [1.0, 1.0])})
+    import builtins
+    import sys
+    monkeypatch.setattr(sys, "path", list(sys.path))
+    real_import = builtins.__import__
+
+    def no_oracle(name, *a, **k):
+        if name == "oracle":
+            raise FileNotFoundError("reference build absent")
+        return real_import(name, *a, **k)
+
+    monkeypatch.setattr(builtins, "__import__", no_oracle)
+    out = b.config0_to_1e8(E, _I, reps=2)
+    assert out["eps"] == 1e-8 and calls == ["close"]
+    for name in ("fp64", "fp32_refined", "bf16_values_refined"):
+        assert out[name]["status"] == 0
+        if out["oracle_objective"] is not None:
+            assert "objective_rel_err_vs_oracle" in out[name]
+    assert "unavailable" in out["reference_gpupdlp"]
+    json.dumps(out, allow_nan=False)
