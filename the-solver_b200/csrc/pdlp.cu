@@ -1,5 +1,6 @@
 // Restarted adaptive PDLP behind sankhya_b200_pdlp_solve, in FP64 or with
-// FP32 inner iterations inside an FP64 iterative-refinement loop (FP32_REFINE).
+// FP32 inner iterations inside an FP64 iterative-refinement loop (FP32_REFINE; with
+// bf16 matrix values under the FP32 iterations, BF16_REFINE).
 //
 // The algorithm is the reference's GpuPdlp (src/cuda/GpuPdlp.cpp:179-534,
 // src/cuda/PdlpKernels.cu:71-518): power-iteration ||A||_2, eta = 0.9/||A||,
@@ -35,8 +36,10 @@
 // rounding stays relative to the step, not to the iterate, and the loop takes the
 // FP64 loop's iterations and reaches its accuracy (plain FP32 iterates stall the
 // adaptive step: its interaction term dy'A dx is a difference of O(1) FP32
-// products). The Halpern loop and the fixed step keep an FP32 phase to 1e-4
-// followed by an FP64 finish.
+// products). BF16_REFINE rounds the scaled matrix values of those iterations to
+// bf16 (each widened to FP32 as the fused kernel loads it); the center's products
+// and the residuals keep the FP64 values. The Halpern loop and the fixed step keep
+// an FP32 phase to 1e-4 followed by an FP64 finish.
 // (A Gleixner-Steffy-Wolter correction LP with scaled residuals was tried first:
 // it re-solves the slow tail of PDLP at every pass and made no progress on boxed
 // LPs; re-centering without scaling keeps the restart schedule running instead.)
