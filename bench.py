@@ -399,6 +399,59 @@ def config0_to_1e8(E, I, reps=3):
     return out
 
 
+def run_plain_pdhg(args):
+    """Config 1: the plain fixed-step FP64 PDHG the reference's GPU code runs
+    (sankhya_cuda_qp_pdhg_preconditioned, steps 0.9 / (1 + |A| mass), no restarts or
+    adaptive step; this engine's kernels) from zero for growing iteration budgets, each
+    point's objective error against the oracle value and its largest row violation
+    (relative to 1 + max |row bound|), beside the restarted PDLP with FP32 iterations
+    refined in FP64 stopped at 1e-6 relative KKT. Prints one JSON line."""
+    E = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
+    I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    import scipy.sparse as sp
+    inst = I.lp_config1(SEED)
+    m, n = inst["m"], inst["n"]
+    A = E.Matrix.from_instance(inst)
+    Ah = sp.csr_matrix((inst["val"], inst["idx"], inst["ptr"]), shape=(m, n))
+    rows = np.repeat(np.arange(m), np.diff(inst["ptr"]))
+    rmass = np.bincount(rows, weights=np.abs(inst["val"]), minlength=m)
+    cmass = np.bincount(inst["idx"], weights=np.abs(inst["val"]), minlength=n)
+    ps, ds = 0.9 / (1 + cmass), 0.9 / (1 + rmass)
+    oracle = oracle_objective()
+    bscale = 1.0 + max(np.abs(inst["rl"]).max(), np.abs(inst["ru"]).max())
+
+    def quality(x):
+        act = Ah @ x
+        viol = max(0.0, float(np.max(inst["rl"] - act)), float(np.max(act - inst["ru"])))
+        obj = float(np.dot(inst["c"], x))
+        q = {"objective": obj, "row_violation_rel": viol / bscale}
+        if oracle is not None:
+            q["objective_rel_err_vs_oracle"] = abs(obj - oracle) / (1.0 + abs(oracle))
+        return q
+
+    out = {"metric": "plain fixed-step FP64 PDHG vs restarted PDLP (FP32 refined), config 1", "unit": "s",
+           "higher_is_better": False, "data": "synthetic", "dtype": "f64",
+           "workload": "lp_config1: m=1,000,000, n=2,000,000, 20M nnz", "oracle_objective": oracle, "plain": []}
+    host = {k: np.ascontiguousarray(inst[k]) for k in ("c", "rl", "ru", "cl", "cu")}
+    for its in (20_000, 60_000, 180_000):
+        s = E.settings(its, its, 0.0, 0.0, 1.0, 1e-12)
+        t0 = time.perf_counter()
+        rc, x, _, r = E.pdhg(A, host, s, primal_steps=ps, dual_steps=ds, entry="preconditioned")
+        wall = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(E.last_error())
+        out["plain"].append({"iterations": its, "seconds": round(wall, 2), **quality(x)})
+    p = E.pdlp_default_settings()
+    p.eps_optimal, p.precision, p.time_limit, p.max_iterations = 1e-6, E.FP32_REFINE, 120.0, 20_000_000
+    t0 = time.perf_counter()
+    rc, x, _, r = E.pdlp_solve(A, inst, p)
+    wall = time.perf_counter() - t0
+    out["pdlp_fp32_refined_1e-6"] = {"seconds": round(wall, 2), "status": r["status"], "iterations": r["iterations"],
+                                     **quality(x)}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def _finite(v):
     """A float for the JSON line, or None where it is not finite (NaN is not JSON)."""
     v = float(v)
@@ -734,7 +787,11 @@ def main():
     ap.add_argument("--nodes-only", action="store_true", help="with --batches: the shared-matrix node batch only")
     ap.add_argument("--qp", action="store_true", help="convex QP workload instead of the headline line")
     ap.add_argument("--pdlp-compare", action="store_true", help="adaptive versus Halpern PDLP on four instances")
+    ap.add_argument("--plain-pdhg", action="store_true",
+                    help="plain fixed-step FP64 PDHG against the restarted refined PDLP on config 1")
     args = ap.parse_args()
+    if args.plain_pdhg:
+        return run_plain_pdhg(args)
     if args.pdlp_compare:
         return run_pdlp_compare(args)
     if args.batches:
