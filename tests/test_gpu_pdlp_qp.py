@@ -2,8 +2,8 @@
 QPs, and seeded convex QPs against the reference's own sk_solve QP answer (its first-
 order loop finished by its active-set polish, certified by its sk_verify to ~1e-14;
 c/src/sk_solve.c:908-954), for the diagonal Hessian (exact prox) and the general
-Hessian (gradient step, curvature in the adaptive step), in FP64 and with FP32
-iterations refined in FP64."""
+Hessian (gradient step, curvature in the adaptive step), in FP64, with FP32
+iterations refined in FP64, and with those iterations over bf16 values of A."""
 import numpy as np
 import pytest
 
@@ -32,7 +32,7 @@ def _diag_hessian_inst(inst):
 
 
 @pytest.mark.parametrize("form", ["diagonal", "hessian"])
-@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE"])
+@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE", "BF16_REFINE"])
 def test_hand_solved_qps(engine, instances, form, precision):
     # min x^2 - 4x, 0 <= x <= 10 (row and column): x = 2, objective -4 (the reference's
     # diagonal_qp_smoke answer); and min x'Qx/2 - 1'x with Q = [[2, 1], [1, 2]], x >= 0,
@@ -65,7 +65,7 @@ def test_hand_solved_qps(engine, instances, form, precision):
 
 
 @pytest.mark.parametrize("form", ["diagonal", "hessian"])
-@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE"])
+@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE", "BF16_REFINE"])
 def test_qp_matches_reference_sk_solve(engine, oracle, instances, form, precision):
     inst = instances.qp_diag_plus_lowrank(31, 100, 200, a_per_col=3, l_per_col=2)
     ref_inst = inst if form == "hessian" else _diag_hessian_inst(inst)
