@@ -672,6 +672,34 @@ def run_batches(args):
                           round(uneven, 2), "algorithmic_gbs": round(uneven_bytes / uneven / 1e3, 1),
                           "frac_of_hbm": round(uneven_bytes / uneven / 1e3 / peak, 3)},
            "peak_kind": peak_kind}
+
+    # time to the gates: each LP runs sk_solve's loop until its own gates pass (row
+    # violation, step and dual-step tests at 1e-4, checked every 20 iterations), the
+    # reference's stopping rule for that loop; wall time of the whole batch call
+    def to_gates(run, cap):
+        s = E.batch_default_settings()
+        s.max_iterations, s.primal_tol, s.dual_tol = cap, 1e-4, 1e-4
+        run(s)
+        t0 = time.perf_counter()
+        rc, res = run(s)
+        wall = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(E.last_error())
+        its = np.array([r["iterations"] for r in res])
+        return {"seconds": round(wall, 3), "tolerance": 1e-4, "iteration_cap": cap,
+                "converged": int(sum(r["status"] == 0 for r in res)), "lps": len(res),
+                "iterations_median": int(np.median(its)), "iterations_max": int(its.max())}
+
+    def shared_run(s):
+        rc, _, _, res = E.shared_batch_pdhg(A, nodes_n, base["c"], base["rl"], base["ru"], cl, cu, s)
+        return rc, res
+
+    def uneven_run(s):
+        rc, _, _, res = E.batch_pdhg(B3, blk3, rseg3, cseg3, s)
+        return rc, res
+
+    out["node_relaxations"]["to_gates"] = to_gates(shared_run, 50_000)
+    out["uneven_lps"]["to_gates"] = to_gates(uneven_run, 50_000)
     print(json.dumps(out))
     return 0
 
