@@ -452,6 +452,70 @@ def run_plain_pdhg(args):
     return 0
 
 
+def run_polish(args):
+    """Feasibility polishing on config 1 (and config 0): the restarted FP64 PDLP
+    stopped at 1e-4 relative KKT beside the polished solve (gap 1e-4, then 1e-6;
+    primal and dual residual 1e-8), with wall time, the rounds and iterations of each
+    part, and each answer's objective error against the oracle value and largest row
+    violation (relative to 1 + max |row bound|). Prints one JSON line."""
+    E = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
+    I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    import scipy.sparse as sp
+    out = {"metric": "restarted FP64 PDLP with feasibility polishing (primal and dual residual 1e-8)", "unit": "s",
+           "higher_is_better": False, "data": "synthetic", "dtype": "f64"}
+    golden0 = os.path.join(ROOT, "tests", "golden", "simplex_lp_config0.json")
+    cases = [("lp_config1", I.lp_config1(SEED), oracle_objective(), (1e-4, 1e-6)),
+             ("lp_config0", I.lp_config0(0), json.load(open(golden0))["objective"], (1e-4, 1e-8))]
+    for name, inst, oracle, gaps in cases:
+        m, n = inst["m"], inst["n"]
+        A = E.Matrix.from_instance(inst)
+        Ah = sp.csr_matrix((inst["val"], inst["idx"], inst["ptr"]), shape=(m, n))
+        bscale = 1.0 + max(np.abs(inst["rl"]).max(), np.abs(inst["ru"]).max())
+
+        def quality(x, r):
+            act = Ah @ x
+            viol = max(0.0, float(np.max(inst["rl"] - act)), float(np.max(act - inst["ru"])))
+            obj = float(np.dot(inst["c"], x))
+            q = {"status": r["status"], "iterations": r["iterations"], "objective": obj,
+                 "row_violation_rel": viol / bscale, "relative_primal_residual": _finite(r["relative_primal_residual"]),
+                 "relative_dual_residual": _finite(r["relative_dual_residual"]),
+                 "relative_gap": _finite(r["relative_gap"])}
+            if oracle is not None:
+                q["objective_rel_err_vs_oracle"] = abs(obj - oracle) / (1.0 + abs(oracle))
+            return q
+
+        def settings(eps):
+            p = E.pdlp_default_settings()
+            p.eps_optimal, p.time_limit, p.max_iterations = eps, 60.0, 20_000_000
+            return p
+
+        leg = {"workload": f"{name}: m={m:,}, n={n:,}, {int(inst['ptr'][-1]):,} nnz", "oracle_objective": oracle}
+        t0 = time.perf_counter()
+        rc, x, _, r = E.pdlp_solve(A, inst, settings(1e-4))
+        if rc != 0:
+            raise RuntimeError(E.last_error())
+        leg["plain_1e-4"] = {"seconds": round(time.perf_counter() - t0, 2), **quality(x, r)}
+        for gap in gaps:
+            t0 = time.perf_counter()
+            rc, x, _, r, pr = E.pdlp_solve_polished(A, inst, settings(gap))
+            if rc != 0:
+                raise RuntimeError(E.last_error())
+            leg[f"polished_gap_{gap:.0e}"] = {
+                "seconds": round(time.perf_counter() - t0, 2), **quality(x, r),
+                "rounds": pr["rounds"], "main_iterations": pr["main_iterations"],
+                "primal_polish_iterations": pr["primal_iterations"], "dual_polish_iterations": pr["dual_iterations"],
+                "main_seconds": round(pr["main_seconds"], 2), "polish_seconds": round(pr["polish_seconds"], 2),
+                "last_pair": {"relative_primal_residual": _finite(pr["pair_relative_primal_residual"]),
+                              "relative_gap": _finite(pr["pair_relative_gap"]),
+                              "primal_objective": _finite(pr["pair_primal_objective"])},
+                "main_at_last_handover": {"relative_primal_residual": _finite(pr["main_relative_primal_residual"]),
+                                          "relative_gap": _finite(pr["main_relative_gap"])}}
+        out[name] = leg
+        A.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def _finite(v):
     """A float for the JSON line, or None where it is not finite (NaN is not JSON)."""
     v = float(v)
@@ -815,11 +879,15 @@ def main():
     ap.add_argument("--nodes-only", action="store_true", help="with --batches: the shared-matrix node batch only")
     ap.add_argument("--qp", action="store_true", help="convex QP workload instead of the headline line")
     ap.add_argument("--pdlp-compare", action="store_true", help="adaptive versus Halpern PDLP on four instances")
+    ap.add_argument("--polish", action="store_true",
+                    help="feasibility polishing on configs 1 and 0 beside the plain restarted solve")
     ap.add_argument("--plain-pdhg", action="store_true",
                     help="plain fixed-step FP64 PDHG against the restarted refined PDLP on config 1")
     args = ap.parse_args()
     if args.plain_pdhg:
         return run_plain_pdhg(args)
+    if args.polish:
+        return run_polish(args)
     if args.pdlp_compare:
         return run_pdlp_compare(args)
     if args.batches:

@@ -243,6 +243,71 @@ SANKHYA_CUDA_API int sankhya_b200_pdlp_solve_qp(
     const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0,
     double* x_out, double* y_out, SankhyaB200PdlpResult* result);
 
+/* ------------------------------------------------- feasibility polishing */
+
+typedef struct SankhyaB200PolishSettings {
+    int struct_version;          /* 1                                                    */
+    int max_polish_iterations;   /* per polishing solve; 0: as many as the main loop has
+                                    run so far                                           */
+    double start_tolerance;      /* relative KKT at which the main loop first hands over
+                                    (1e-4); each later hand-over is 10x tighter, down to
+                                    the smaller of eps_optimal and polish_tolerance      */
+    double polish_tolerance;     /* relative primal residual of the polished x and
+                                    relative dual residual of the polished y (1e-8)      */
+} SankhyaB200PolishSettings;
+
+SANKHYA_CUDA_API void sankhya_b200_polish_default_settings(SankhyaB200PolishSettings* settings);
+
+typedef struct SankhyaB200PolishResult {
+    int rounds;                  /* hand-overs from the main loop to polishing          */
+    int main_iterations;         /* iterations of the main (restarted adaptive) loop    */
+    int primal_iterations;       /* iterations of the primal polishing solves           */
+    int dual_iterations;         /* iterations of the dual polishing solves             */
+    double main_seconds;
+    double polish_seconds;
+    double main_relative_primal_residual;  /* the main loop's point at the last hand-over */
+    double main_relative_dual_residual;
+    double main_relative_gap;
+    double pair_relative_primal_residual;  /* the last polished pair, scored on the LP     */
+    double pair_relative_dual_residual;
+    double pair_relative_gap;
+    double pair_primal_objective;
+} SankhyaB200PolishResult;
+
+/* Restarted adaptive PDLP with feasibility polishing (no counterpart in the
+   reference, which lists crossover and polishing as not implemented,
+   docs/architecture/PDLP.md:185; the method is the feasibility polishing of
+   PDLP, Applegate et al. 2025). The main loop of sankhya_b200_pdlp_solve runs
+   to start_tolerance; then, on the same scaled matrix, two warm-started solves
+   of easier problems: the primal feasibility problem (the LP with zero cost)
+   from the main loop's x, run until its x meets polish_tolerance in relative
+   primal residual, and the dual feasibility problem (every finite bound moved
+   to 0, so that its dual feasible set is the original LP's) from the main
+   loop's y, run until its y meets polish_tolerance in relative dual residual.
+   The pair (polished x, polished y) is scored on the original LP (result: its
+   relative residuals, gap and objectives); when the pair misses a target (its
+   gap above eps_optimal, or a polishing solve out of iterations) the main loop
+   resumes to a 10x tighter tolerance and polishing repeats, with budgets that
+   grow with the main loop. A polishing solve is skipped when the main loop's
+   point already meets polish_tolerance on its measure. The rounds end when the
+   pair meets its targets, or at the main loop's iteration limit, time limit or
+   cancellation. Status 0: primal and dual residual of the pair <=
+   polish_tolerance and gap <= eps_optimal. Otherwise the answer is whichever
+   of the scored pairs and the main loop's last point misses its targets by
+   the smallest factor (the largest of primal / polish_tolerance, dual /
+   polish_tolerance, gap / eps_optimal). Needs precision FP64 and the
+   adaptive step of algorithm ADAPTIVE; settings and arrays as for
+   sankhya_b200_pdlp_solve; polish NULL takes the defaults; polish_result may
+   be NULL. Returns 0, -1 on invalid input or CUDA error, -2 on a non-finite
+   iterate. */
+SANKHYA_CUDA_API int sankhya_b200_pdlp_solve_polished(
+    const SankhyaCudaCSR* matrix, const double* c,
+    const double* row_lower, const double* row_upper,
+    const double* col_lower, const double* col_upper,
+    const SankhyaB200PdlpSettings* settings, const SankhyaB200PolishSettings* polish,
+    const double* x0, const double* y0, double* x_out, double* y_out,
+    SankhyaB200PdlpResult* result, SankhyaB200PolishResult* polish_result);
+
 /* ------------------------------------------------------- batched LPs */
 
 typedef struct SankhyaB200BatchSettings {

@@ -185,7 +185,8 @@ MIRRORS = {  # ctypes class in the package -> C struct in include/
     "Timing": "SankhyaB200Timing", "LoopResult": "SankhyaB200LoopResult",
     "PdlpSettings": "SankhyaB200PdlpSettings", "PdlpResult": "SankhyaB200PdlpResult",
     "BatchSettings": "SankhyaB200BatchSettings", "BatchResult": "SankhyaB200BatchResult",
-    "GnnSettings": "SankhyaB200GnnSettings",
+    "GnnSettings": "SankhyaB200GnnSettings", "PolishSettings": "SankhyaB200PolishSettings",
+    "PolishResult": "SankhyaB200PolishResult",
 }
 
 
@@ -240,6 +241,50 @@ def test_pdlp_settings_versions(engine, instances):
         rc = L.sankhya_b200_pdlp_solve(C.byref(fake), d(inst["c"]), d(inst["rl"]), d(inst["ru"]), d(inst["cl"]),
                                        d(inst["cu"]), C.byref(s), None, None, d(x), None, C.byref(res))
         assert rc == -1 and message in engine.last_error(), (version, engine.last_error())
+
+
+def test_polishing_settings_checks(engine, instances):
+    """The polishing entry point checks its settings before any device work: the
+    defaults (and NULL polishing settings) reach the device check; another struct
+    version, a non-positive tolerance, a negative budget, or a main loop other than
+    the FP64 adaptive one are refused."""
+    import numpy as np
+    import torch
+    if torch.cuda.is_available():
+        return
+    inst = instances.lp_uniform(1, 8, 12, 2)
+    fake = engine.CSR(inst["m"], inst["n"], int(inst["ptr"][-1]), None, None, None)
+    L = engine.lib()
+    d = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double))
+    p = engine.polish_default_settings()
+    assert (p.struct_version, p.max_polish_iterations, p.start_tolerance, p.polish_tolerance) == (1, 0, 1e-4, 1e-8)
+
+    def call(edit_polish=None, edit_settings=None, null_polish=False):
+        s = engine.pdlp_default_settings()
+        q = engine.polish_default_settings()
+        if edit_polish:
+            edit_polish(q)
+        if edit_settings:
+            edit_settings(s)
+        res, pres = engine.PdlpResult(), engine.PolishResult()
+        pres.rounds = 99
+        x = np.zeros(inst["n"])
+        rc = L.sankhya_b200_pdlp_solve_polished(C.byref(fake), d(inst["c"]), d(inst["rl"]), d(inst["ru"]),
+                                                d(inst["cl"]), d(inst["cu"]), C.byref(s),
+                                                None if null_polish else C.byref(q), None, None, d(x), None,
+                                                C.byref(res), C.byref(pres))
+        assert rc == -1 and res.status == -1 and pres.rounds == 0
+        return engine.last_error()
+
+    assert "device" in call()
+    assert "device" in call(null_polish=True)
+    assert "struct_version" in call(edit_polish=lambda q: setattr(q, "struct_version", 2))
+    for field, value in (("start_tolerance", 0.0), ("polish_tolerance", -1.0), ("polish_tolerance", float("nan")),
+                         ("max_polish_iterations", -1)):
+        assert "invalid polishing settings" in call(edit_polish=lambda q: setattr(q, field, value)), field
+    for field, value in (("precision", engine.FP32_REFINE), ("adaptive_step", 0),
+                         ("algorithm", engine.PDLP_HALPERN)):
+        assert "FP64 adaptive loop" in call(edit_settings=lambda s: setattr(s, field, value)), field
 
 
 def test_headers_compile_as_c_and_cxx_and_every_symbol_links(tmp_path):

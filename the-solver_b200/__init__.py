@@ -38,7 +38,8 @@ EXTENSION_SYMBOLS = (
     "sankhya_b200_lp_pdhg_device_noalloc", "sankhya_b200_gnn_default_settings", "sankhya_b200_gnn_create",
     "sankhya_b200_gnn_destroy", "sankhya_b200_gnn_parameter_count", "sankhya_b200_gnn_get_parameters",
     "sankhya_b200_gnn_set_parameters", "sankhya_b200_gnn_predict", "sankhya_b200_gnn_gradient",
-    "sankhya_b200_gnn_train_step", "sankhya_b200_csr_transpose",
+    "sankhya_b200_gnn_train_step", "sankhya_b200_csr_transpose", "sankhya_b200_polish_default_settings",
+    "sankhya_b200_pdlp_solve_polished",
 )
 
 _lib = None
@@ -132,6 +133,25 @@ class PdlpResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PolishSettings(C.Structure):
+    """SankhyaB200PolishSettings."""
+    _fields_ = [("struct_version", C.c_int), ("max_polish_iterations", C.c_int),
+                ("start_tolerance", C.c_double), ("polish_tolerance", C.c_double)]
+
+
+class PolishResult(C.Structure):
+    """SankhyaB200PolishResult."""
+    _fields_ = [("rounds", C.c_int), ("main_iterations", C.c_int), ("primal_iterations", C.c_int),
+                ("dual_iterations", C.c_int), ("main_seconds", C.c_double), ("polish_seconds", C.c_double),
+                ("main_relative_primal_residual", C.c_double), ("main_relative_dual_residual", C.c_double),
+                ("main_relative_gap", C.c_double), ("pair_relative_primal_residual", C.c_double),
+                ("pair_relative_dual_residual", C.c_double), ("pair_relative_gap", C.c_double),
+                ("pair_primal_objective", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class BatchSettings(C.Structure):
     """SankhyaB200BatchSettings."""
     _fields_ = [("struct_version", C.c_int), ("max_iterations", C.c_int), ("check_every", C.c_int),
@@ -192,6 +212,12 @@ def _declare(L):
     if hasattr(L, "sankhya_b200_pdlp_solve_qp"):
         L.sankhya_b200_pdlp_solve_qp.argtypes = [P(CSR), P(CSR), dptr, dptr, dptr, dptr, dptr, dptr,
                                                  P(PdlpSettings), dptr, dptr, dptr, dptr, P(PdlpResult)]
+    if hasattr(L, "sankhya_b200_pdlp_solve_polished"):
+        L.sankhya_b200_polish_default_settings.argtypes = [P(PolishSettings)]
+        L.sankhya_b200_polish_default_settings.restype = None
+        L.sankhya_b200_pdlp_solve_polished.argtypes = [P(CSR), dptr, dptr, dptr, dptr, dptr, P(PdlpSettings),
+                                                       P(PolishSettings), dptr, dptr, dptr, dptr, P(PdlpResult),
+                                                       P(PolishResult)]
     if hasattr(L, "sankhya_b200_batch_pdhg"):
         L.sankhya_b200_batch_default_settings.argtypes = [P(BatchSettings)]
         L.sankhya_b200_batch_default_settings.restype = None
@@ -383,6 +409,30 @@ def pdlp_solve_qp(matrix: Matrix, inst, s: PdlpSettings | None = None, hessian: 
                                       _p(qd), _p(c), _p(rl), _p(ru), _p(cl), _p(cu), C.byref(s), _p(_d(x0)),
                                       _p(_d(y0)), _p(x), _p(y), C.byref(res))
     return rc, x, y, res.as_dict()
+
+
+def polish_default_settings() -> PolishSettings:
+    p = PolishSettings()
+    lib().sankhya_b200_polish_default_settings(C.byref(p))
+    return p
+
+
+def pdlp_solve_polished(matrix: Matrix, inst, s: PdlpSettings | None = None, polish: PolishSettings | None = None,
+                        x0=None, y0=None, want_dual=True, **over):
+    """sankhya_b200_pdlp_solve_polished: the restarted FP64 solve with feasibility
+    polishing; returns (rc, x, y, result, polish_result)."""
+    L = lib()
+    s = s or pdlp_default_settings()
+    get = lambda k: _d(over[k]) if k in over else _d(inst[k])
+    c, rl, ru, cl, cu = get("c"), get("rl"), get("ru"), get("cl"), get("cu")
+    n, m = matrix.handle.cols, matrix.handle.rows
+    x = np.zeros(n)
+    y = np.zeros(m) if want_dual else None
+    res, pres = PdlpResult(), PolishResult()
+    rc = L.sankhya_b200_pdlp_solve_polished(C.byref(matrix.handle), _p(c), _p(rl), _p(ru), _p(cl), _p(cu),
+                                            C.byref(s), C.byref(polish) if polish is not None else None,
+                                            _p(_d(x0)), _p(_d(y0)), _p(x), _p(y), C.byref(res), C.byref(pres))
+    return rc, x, y, res.as_dict(), pres.as_dict()
 
 
 def scale_factors(matrix: Matrix, scaling: int, ruiz_iterations: int = 100, ruiz_tolerance: float = 1e-2):

@@ -939,6 +939,16 @@ __global__ void k_widen(int n, int m, const float* __restrict__ x32, const float
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) y[i] = static_cast<double>(y32[i]);
 }
 
+// The bounds of the dual feasibility problem: every finite bound moved to 0,
+// infinite ones kept, so the problem's dual feasible set is the original LP's.
+__global__ void k_homogeneous(int len, const double* __restrict__ lo, const double* __restrict__ hi,
+                              double* __restrict__ lo0, double* __restrict__ hi0) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += blockDim.x * gridDim.x) {
+        lo0[i] = isfinite(lo[i]) ? 0.0 : lo[i];
+        hi0[i] = isfinite(hi[i]) ? 0.0 : hi[i];
+    }
+}
+
 __global__ void k_narrow(long long n, const double* __restrict__ in, float* __restrict__ out) {
     for (long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; j < n;
          j += static_cast<long long>(blockDim.x) * gridDim.x)
@@ -957,9 +967,16 @@ double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Which relative KKT measures end a loop: all three (the default), or only the
+// primal residual / only the dual residual (the polishing solves).
+constexpr int kPrimalMeasure = 1, kDualMeasure = 2, kAllMeasures = 7;
+
 struct Kkt {
     double primal = 1, dual = 1, gap = 1, pobj = 0, dobj = 0, pmove = 0, dmove = 0;
     double worst() const { return std::max(std::max(primal, dual), gap); }
+    double on(int measure) const {
+        return measure == kPrimalMeasure ? primal : measure == kDualMeasure ? dual : worst();
+    }
 };
 
 Kkt to_kkt(const double* r, double cost_norm, double bound_norm) {
@@ -1133,6 +1150,7 @@ struct LoopParams {
     bool halpern = false; // reflected restarted Halpern PDHG instead of GpuPdlp's loop
     int (*cancel)(void*) = nullptr;  // polled after each window; non-zero stops the solve
     void* cancel_context = nullptr;
+    int measure = kAllMeasures;  // what must reach eps (restarts always use all three)
 };
 
 // The FP64 side of the centered FP32 loop: the scaled FP64 problem, the center
@@ -1599,14 +1617,16 @@ struct Core {
             out->eta = h[16 + 8];
             out->accept_count = h[16 + 9];
             out->updates = h[16 + 10];
-            const bool average_better = average.worst() < current.worst();
+            const bool average_better = lp.measure == kAllMeasures ? average.worst() < current.worst()
+                                                                   : average.on(lp.measure) < current.on(lp.measure);
             out->best = average_better ? average : current;
             const Kkt best = out->best;
             if (!std::isfinite(current.primal) && !std::isfinite(average.primal)) {
                 out->numeric = true;
                 break;
             }
-            if (best.primal <= lp.eps && best.dual <= lp.eps && best.gap <= lp.eps) {
+            if (lp.measure == kAllMeasures ? best.primal <= lp.eps && best.dual <= lp.eps && best.gap <= lp.eps
+                                           : best.on(lp.measure) <= lp.eps) {
                 if (average_better) {
                     B200_TRY(cudaMemcpyAsync(x, x_avg, nb, cudaMemcpyDeviceToDevice, stream), "copy");
                     B200_TRY(cudaMemcpyAsync(y, y_avg, mb, cudaMemcpyDeviceToDevice, stream), "copy");
@@ -1699,14 +1719,191 @@ __global__ void k_scale_diag(int n, const double* __restrict__ q, const double* 
         out[j] = (q[j] * Cs[j]) * Cs[j];
 }
 
+// Feasibility polishing around the FP64 main loop (sankhya_b200_pdlp_solve_polished).
+// hi holds the start point on entry and the answer on return (scaled space); lp is the
+// main loop's parameters with the scaled problem's norms; stats receives the loop
+// counters of every solve and the answer's relative KKT on the original problem.
+int run_polished(const Scaled& sc, Core<double>& hi, const LoopParams& lp, const SankhyaB200PdlpSettings& s,
+                 const SankhyaB200PolishSettings& ps, double* host, LoopStats* stats, SankhyaB200PolishResult* pr,
+                 int* launches) {
+    cudaStream_t stream = hi.stream;
+    const int n = hi.n, m = hi.m;
+    const size_t nb = sizeof(double) * static_cast<size_t>(std::max(n, 1));
+    const size_t mb = sizeof(double) * static_cast<size_t>(std::max(m, 1));
+    const size_t nd = (nb + 255) / 256 * 256, md = (mb + 255) / 256 * 256;
+    DevBuf buf;
+    if (buf.alloc(5 * nd + 4 * md, "cudaMalloc polishing data")) return -1;
+    char* base = buf.as<char>();
+    double* zero_c = reinterpret_cast<double*>(base);
+    double* cl0 = reinterpret_cast<double*>(base + nd);
+    double* cu0 = reinterpret_cast<double*>(base + 2 * nd);
+    double* xp = reinterpret_cast<double*>(base + 3 * nd);   // the pair being scored
+    double* xb = reinterpret_cast<double*>(base + 4 * nd);   // the best pair so far
+    double* rl0 = reinterpret_cast<double*>(base + 5 * nd);
+    double* ru0 = reinterpret_cast<double*>(base + 5 * nd + md);
+    double* yd = reinterpret_cast<double*>(base + 5 * nd + 2 * md);
+    double* yb = reinterpret_cast<double*>(base + 5 * nd + 3 * md);
+    B200_TRY(cudaMemsetAsync(zero_c, 0, nb, stream), "zero");
+    k_homogeneous<<<eg(n), kThreads, 0, stream>>>(n, sc.cl, sc.cu, cl0, cu0);
+    k_homogeneous<<<eg(m), kThreads, 0, stream>>>(m, sc.rl, sc.ru, rl0, ru0);
+    *launches += 2;
+    Core<double> pol;
+    pol.stream = stream;
+    pol.host = host;
+    if (pol.allocate(n, m, sc.sms)) return -1;
+    const auto d2d = cudaMemcpyDeviceToDevice;
+
+    // how far a point misses the targets (<= 1: met)
+    const auto miss = [&](const Kkt& k) {
+        return std::max(std::max(k.primal, k.dual) / ps.polish_tolerance, k.gap / s.eps_optimal);
+    };
+    LoopStats& acc = *stats;
+    double tol = std::max(ps.start_tolerance, s.eps_optimal);
+    long long main_used = 0;
+    bool have_pair = false, met = false;
+    Kkt best_pair;
+    for (;;) {
+        // the main loop, resumed from its own last point with its step and weight
+        const double t_main = now_s();
+        LoopParams ml = lp;
+        ml.eps = tol;
+        ml.max_iterations = s.max_iterations - main_used;
+        if (main_used > 0) {
+            ml.omega0 = acc.omega;
+            ml.eta0 = acc.eta;
+        }
+        LoopStats ms;
+        if (hi.run(ml, &ms)) return -1;
+        pr->main_seconds += now_s() - t_main;
+        main_used += ms.iterations;
+        acc.iterations += ms.iterations;
+        acc.restarts += ms.restarts;
+        acc.syncs += ms.syncs;
+        acc.updates += ms.updates;
+        acc.accept_count += ms.accept_count;
+        acc.eta = ms.eta;
+        acc.omega = ms.omega;
+        acc.best = ms.best;
+        acc.numeric = ms.numeric;
+        acc.timed_out = ms.timed_out;
+        acc.cancelled = ms.cancelled;
+        if (ms.numeric || ms.timed_out || ms.cancelled) break;
+        ++pr->rounds;
+        pr->main_iterations = static_cast<int>(std::min<long long>(main_used, 2147483647LL));
+        pr->main_relative_primal_residual = ms.best.primal;
+        pr->main_relative_dual_residual = ms.best.dual;
+        pr->main_relative_gap = ms.best.gap;
+
+        const double t_pol = now_s();
+        const long long budget = ps.max_polish_iterations > 0
+                                     ? ps.max_polish_iterations
+                                     : std::max<long long>(main_used, lp.restart_period);
+        LoopParams pl = lp;
+        pl.eps = ps.polish_tolerance;
+        pl.max_iterations = budget;
+        pl.omega0 = ms.omega;
+        pl.eta0 = ms.eta;
+        // primal feasibility problem (zero cost) from the main loop's x, dual at zero
+        B200_TRY(cudaMemcpyAsync(xp, hi.x, nb, d2d, stream), "copy");
+        if (!(ms.best.primal <= ps.polish_tolerance)) {
+            pol.set_problem(sc.A, sc.AT, zero_c, sc.cl, sc.cu, sc.rl, sc.ru);
+            B200_TRY(cudaMemcpyAsync(pol.x, hi.x, nb, d2d, stream), "copy");
+            B200_TRY(cudaMemsetAsync(pol.y, 0, mb, stream), "zero");
+            pl.cost_norm = 0.0;
+            pl.bound_norm = lp.bound_norm;
+            pl.measure = kPrimalMeasure;
+            LoopStats fs;
+            if (pol.run(pl, &fs)) return -1;
+            pr->primal_iterations += static_cast<int>(fs.iterations);
+            acc.iterations += fs.iterations;
+            acc.syncs += fs.syncs;
+            acc.timed_out = acc.timed_out || fs.timed_out;
+            acc.cancelled = acc.cancelled || fs.cancelled;
+            if (fs.numeric) {
+                acc.numeric = true;
+                break;
+            }
+            B200_TRY(cudaMemcpyAsync(xp, pol.x, nb, d2d, stream), "copy");
+        }
+        // dual feasibility problem (finite bounds at zero) from the main loop's y, primal at zero
+        B200_TRY(cudaMemcpyAsync(yd, hi.y, mb, d2d, stream), "copy");
+        if (!(ms.best.dual <= ps.polish_tolerance) && !acc.timed_out && !acc.cancelled) {
+            pol.set_problem(sc.A, sc.AT, sc.c, cl0, cu0, rl0, ru0);
+            B200_TRY(cudaMemsetAsync(pol.x, 0, nb, stream), "zero");
+            B200_TRY(cudaMemcpyAsync(pol.y, hi.y, mb, d2d, stream), "copy");
+            pl.cost_norm = lp.cost_norm;
+            pl.bound_norm = 0.0;
+            pl.measure = kDualMeasure;
+            LoopStats fs;
+            if (pol.run(pl, &fs)) return -1;
+            pr->dual_iterations += static_cast<int>(fs.iterations);
+            acc.iterations += fs.iterations;
+            acc.syncs += fs.syncs;
+            acc.timed_out = acc.timed_out || fs.timed_out;
+            acc.cancelled = acc.cancelled || fs.cancelled;
+            if (fs.numeric) {
+                acc.numeric = true;
+                break;
+            }
+            B200_TRY(cudaMemcpyAsync(yd, pol.y, mb, d2d, stream), "copy");
+        }
+        pr->polish_seconds += now_s() - t_pol;
+        // the pair, scored on the original problem
+        pol.set_problem(sc.A, sc.AT, sc.c, sc.cl, sc.cu, sc.rl, sc.ru);
+        B200_TRY(cudaMemcpyAsync(pol.x, xp, nb, d2d, stream), "copy");
+        B200_TRY(cudaMemcpyAsync(pol.x_restart, xp, nb, d2d, stream), "copy");
+        B200_TRY(cudaMemcpyAsync(pol.y, yd, mb, d2d, stream), "copy");
+        B200_TRY(cudaMemcpyAsync(pol.y_restart, yd, mb, d2d, stream), "copy");
+        k_init_state<<<1, 1, 0, stream>>>(pol.st, ms.eta, ms.omega, ms.eta, ms.eta);
+        ++pol.launches;
+        pol.residuals(pol.x, pol.y, nullptr, nullptr, pol.res, 0);
+        B200_TRY(cudaMemcpyAsync(host, pol.res, 16 * sizeof(double), cudaMemcpyDeviceToHost, stream), "copy");
+        B200_TRY(cudaStreamSynchronize(stream), "polishing");
+        ++acc.syncs;
+        const Kkt pair = to_kkt(host, lp.cost_norm, lp.bound_norm);
+        pr->pair_relative_primal_residual = pair.primal;
+        pr->pair_relative_dual_residual = pair.dual;
+        pr->pair_relative_gap = pair.gap;
+        pr->pair_primal_objective = pair.pobj;
+        if (!have_pair || miss(pair) < miss(best_pair)) {
+            B200_TRY(cudaMemcpyAsync(xb, xp, nb, d2d, stream), "copy");
+            B200_TRY(cudaMemcpyAsync(yb, yd, mb, d2d, stream), "copy");
+            best_pair = pair;
+            have_pair = true;
+        }
+        met = pair.primal <= ps.polish_tolerance && pair.dual <= ps.polish_tolerance && pair.gap <= s.eps_optimal;
+        if (met) break;
+        // not yet: the main loop resumes to a tighter tolerance (at the floor its own
+        // point meets both polishing measures and the gap, and the pair is that point)
+        if (acc.timed_out || acc.cancelled || !ms.converged || main_used >= s.max_iterations) break;
+        tol = std::max(tol * 0.1, std::min(s.eps_optimal, ps.polish_tolerance));
+    }
+    *launches += pol.launches;
+    acc.converged = met;
+    // the answer: the pair that met the targets, else the closer of the best pair and
+    // the main loop's last point (hi.x / hi.y, scored acc.best)
+    if (have_pair && (met || acc.numeric || miss(best_pair) < miss(acc.best))) {
+        B200_TRY(cudaMemcpyAsync(hi.x, xb, nb, d2d, stream), "copy");
+        B200_TRY(cudaMemcpyAsync(hi.y, yb, mb, d2d, stream), "copy");
+        acc.best = best_pair;
+        acc.numeric = false;
+    }
+    B200_TRY(cudaStreamSynchronize(stream), "polishing");
+    return 0;
+}
+
 // The LP and QP solve: minimize c'x (+ x'Q x / 2) over rl <= A x <= ru, cl <= x <= cu,
 // with Q a general symmetric Hessian (hessian, full CSR) or a diagonal (qdiag).
 int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, const double* qdiag, const double* c,
                const double* row_lower, const double* row_upper, const double* col_lower, const double* col_upper,
                const SankhyaB200PdlpSettings* settings, const double* x0, const double* y0, double* x_out,
-               double* y_out, SankhyaB200PdlpResult* result) {
+               double* y_out, SankhyaB200PdlpResult* result, bool polishing = false,
+               const SankhyaB200PolishSettings* polish = nullptr, SankhyaB200PolishResult* polish_result = nullptr) {
     clear_error();
     (void)cudaGetLastError();  // a caller's earlier non-sticky error is not ours
+    SankhyaB200PolishResult local_pr;
+    if (!polish_result) polish_result = &local_pr;
+    std::memset(polish_result, 0, sizeof(*polish_result));
     if (!result) return fail_msg("null result");
     std::memset(result, 0, sizeof(*result));
     result->status = -1;
@@ -1749,6 +1946,19 @@ int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, cons
         return fail_msg("the QP solve runs the adaptive step of the restarted loop");
     if (s.precision == SANKHYA_B200_BF16_REFINE && (s.algorithm != SANKHYA_B200_PDLP_ADAPTIVE || !s.adaptive_step))
         return fail_msg("BF16_REFINE runs the adaptive step of the restarted loop");
+    SankhyaB200PolishSettings ps;
+    sankhya_b200_polish_default_settings(&ps);
+    if (polishing) {
+        if (polish) {
+            if (polish->struct_version != 1) return fail_msg("unsupported polishing settings struct_version");
+            ps = *polish;
+        }
+        if (!(ps.start_tolerance > 0.0) || !(ps.polish_tolerance > 0.0) || ps.max_polish_iterations < 0)
+            return fail_msg("invalid polishing settings");
+        if (quadratic || s.precision != SANKHYA_B200_FP64 || s.algorithm != SANKHYA_B200_PDLP_ADAPTIVE ||
+            !s.adaptive_step)
+            return fail_msg("polishing runs the FP64 adaptive loop of an LP");
+    }
     for (int j = 0; j < n; ++j)
         if (!std::isfinite(c[j]) || std::isnan(col_lower[j]) || std::isnan(col_upper[j]) || col_lower[j] > col_upper[j])
             return fail_msg("invalid cost or column bound");
@@ -1847,7 +2057,11 @@ int pdlp_solve(const SankhyaCudaCSR* matrix, const SankhyaCudaCSR* hessian, cons
         lp.max_iterations = s.max_iterations;
         lp.cost_norm = cost_norm;
         lp.bound_norm = bound_norm;
-        if (hi.run(lp, &stats)) return -1;
+        if (polishing) {
+            if (run_polished(sc, hi, lp, s, ps, hs.p, &stats, polish_result, &launches)) return -1;
+        } else if (hi.run(lp, &stats)) {
+            return -1;
+        }
         launches += hi.launches;
     } else if (lp.adaptive && !lp.halpern) {
         // ------------------------- FP32 iterations around an FP64 center, refined at restarts
@@ -2057,6 +2271,26 @@ extern "C" int sankhya_b200_pdlp_solve_qp(const SankhyaCudaCSR* matrix, const Sa
                                           double* x_out, double* y_out, SankhyaB200PdlpResult* result) {
     return b200::pdlp_solve(matrix, hessian, quadratic_diagonal, c, row_lower, row_upper, col_lower, col_upper,
                             settings, x0, y0, x_out, y_out, result);
+}
+
+extern "C" void sankhya_b200_polish_default_settings(SankhyaB200PolishSettings* s) {
+    if (!s) return;
+    std::memset(s, 0, sizeof(*s));
+    s->struct_version = 1;
+    s->max_polish_iterations = 0;
+    s->start_tolerance = 1e-4;
+    s->polish_tolerance = 1e-8;
+}
+
+extern "C" int sankhya_b200_pdlp_solve_polished(const SankhyaCudaCSR* matrix, const double* c,
+                                                const double* row_lower, const double* row_upper,
+                                                const double* col_lower, const double* col_upper,
+                                                const SankhyaB200PdlpSettings* settings,
+                                                const SankhyaB200PolishSettings* polish, const double* x0,
+                                                const double* y0, double* x_out, double* y_out,
+                                                SankhyaB200PdlpResult* result, SankhyaB200PolishResult* polish_result) {
+    return b200::pdlp_solve(matrix, nullptr, nullptr, c, row_lower, row_upper, col_lower, col_upper, settings, x0,
+                            y0, x_out, y_out, result, true, polish, polish_result);
 }
 
 extern "C" int sankhya_b200_scale_factors(const SankhyaCudaCSR* matrix, int scaling, int ruiz_iterations,
