@@ -1151,6 +1151,7 @@ struct LoopParams {
     int (*cancel)(void*) = nullptr;  // polled after each window; non-zero stops the solve
     void* cancel_context = nullptr;
     int measure = kAllMeasures;  // what must reach eps (restarts always use all three)
+    bool fixed_weight = false;   // keep omega0 at restarts (the polishing solves)
 };
 
 // The FP64 side of the centered FP32 loop: the scaled FP64 problem, the center
@@ -1667,7 +1668,7 @@ struct Core {
             mu_at_restart = mu;
             mu_previous = std::numeric_limits<double>::infinity();
             ++out->restarts;
-            if (best.pmove > 1e-14 && best.dmove > 1e-14) {
+            if (!lp.fixed_weight && best.pmove > 1e-14 && best.dmove > 1e-14) {
                 const double target = best.dmove / best.pmove;
                 const double updated = std::exp(kSmoothing * std::log(target) + (1.0 - kSmoothing) * std::log(omega));
                 if (std::isfinite(updated)) omega = std::min(kMaxWeight, std::max(kMinWeight, updated));
@@ -1798,11 +1799,18 @@ int run_polished(const Scaled& sc, Core<double>& hi, const LoopParams& lp, const
         const long long budget = ps.max_polish_iterations > 0
                                      ? ps.max_polish_iterations
                                      : std::max<long long>(main_used, lp.restart_period);
+        // Both polishing solves run restarted PDHG with the safe constant step 0.9 / ||A||_2
+        // and the main loop's primal weight held: such PDHG started at z0 stays within the
+        // weighted distance from z0 to the solution set, so the polished point stays near
+        // the main loop's (and near its objective). The adaptive step loses that bound on
+        // a zero-cost problem, where its interaction term starts near zero and lets the
+        // step grow to its cap.
         LoopParams pl = lp;
         pl.eps = ps.polish_tolerance;
         pl.max_iterations = budget;
         pl.omega0 = ms.omega;
-        pl.eta0 = ms.eta;
+        pl.adaptive = false;
+        pl.fixed_weight = true;
         // primal feasibility problem (zero cost) from the main loop's x, dual at zero
         B200_TRY(cudaMemcpyAsync(xp, hi.x, nb, d2d, stream), "copy");
         if (!(ms.best.primal <= ps.polish_tolerance)) {
