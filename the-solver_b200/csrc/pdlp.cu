@@ -43,6 +43,14 @@
 // (A Gleixner-Steffy-Wolter correction LP with scaled residuals was tried first:
 // it re-solves the slow tail of PDLP at every pass and made no progress on boxed
 // LPs; re-centering without scaling keeps the restart schedule running instead.)
+//
+// Feasibility polishing (sankhya_b200_pdlp_solve_polished, run_polished): PDLP's
+// published polishing (Applegate et al. 2025) around the FP64 loop, on the same
+// scaled matrix and the same Core: a zero-cost primal feasibility solve from the
+// loop's x and a dual feasibility solve (finite bounds at 0) from its y, each ended
+// by its own residual alone (LoopParams::measure), the pair scored on the LP by the
+// window-end residual kernels, and the loop resumed 10x tighter until the pair's
+// gap meets the target.
 #include "engine.cuh"
 
 #include <cstddef>
