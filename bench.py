@@ -460,6 +460,12 @@ def run_polish(args):
     violation (relative to 1 + max |row bound|). Prints one JSON line."""
     E = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
     I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    print(json.dumps(polish_legs(E, I)), flush=True)
+    return 0
+
+
+def polish_legs(E, I, time_limit=60.0):
+    """The legs of run_polish for an engine module E and an instance module I."""
     import scipy.sparse as sp
     out = {"metric": "restarted FP64 PDLP with feasibility polishing (primal and dual residual 1e-8)", "unit": "s",
            "higher_is_better": False, "data": "synthetic", "dtype": "f64"}
@@ -486,7 +492,7 @@ def run_polish(args):
 
         def settings(eps):
             p = E.pdlp_default_settings()
-            p.eps_optimal, p.time_limit, p.max_iterations = eps, 60.0, 20_000_000
+            p.eps_optimal, p.time_limit, p.max_iterations = eps, time_limit, 20_000_000
             return p
 
         leg = {"workload": f"{name}: m={m:,}, n={n:,}, {int(inst['ptr'][-1]):,} nnz", "oracle_objective": oracle}
@@ -512,8 +518,7 @@ def run_polish(args):
                                           "relative_gap": _finite(pr["main_relative_gap"])}}
         out[name] = leg
         A.close()
-    print(json.dumps(out), flush=True)
-    return 0
+    return out
 
 
 def _finite(v):

@@ -196,3 +196,63 @@ def test_config0_leg_reports_each_mode_against_the_simplex(monkeypatch):
             assert "objective_rel_err_vs_oracle" in out[name]
     assert "unavailable" in out["reference_gpupdlp"]
     json.dumps(out, allow_nan=False)
+
+
+def test_polish_legs_report_plain_and_polished_answers(monkeypatch):
+    """The --polish legs: per instance the plain 1e-4 solve and one polished solve per
+    gap target, each with its quality against the instance (row violation, objective
+    error against the oracle value) and the polishing counters, as strict JSON."""
+    b = _bench()
+    monkeypatch.setattr(b, "oracle_objective", lambda: -3.0)
+    solves = []
+
+    def tiny(seed):
+        # one row x0 + x1 in [1, 2], boxes [0, 10]
+        return {"m": 1, "n": 2, "ptr": np.array([0, 2]), "idx": np.array([0, 1]), "val": np.array([1.0, 1.0]),
+                "c": np.array([-1.0, -2.0]), "rl": np.array([1.0]), "ru": np.array([2.0]),
+                "cl": np.zeros(2), "cu": np.full(2, 10.0)}
+
+    class _I:
+        lp_config1 = staticmethod(tiny)
+        lp_config0 = staticmethod(tiny)
+
+    class _E:
+        class Matrix:
+            @staticmethod
+            def from_instance(inst):
+                class _M:
+                    def close(self):
+                        solves.append("close")
+                return _M()
+
+        def pdlp_default_settings(self):
+            return _Settings()
+
+        def pdlp_solve(self, A, inst, s):
+            solves.append(("plain", s.eps_optimal))
+            r = {"status": 0, "iterations": 64, "relative_primal_residual": 1e-5, "relative_dual_residual": 0.0,
+                 "relative_gap": 9e-5}
+            return 0, np.array([0.0, 2.1]), np.zeros(1), r
+
+        def pdlp_solve_polished(self, A, inst, s):
+            solves.append(("polished", s.eps_optimal))
+            r = {"status": 0, "iterations": 192, "relative_primal_residual": 0.0, "relative_dual_residual": 0.0,
+                 "relative_gap": s.eps_optimal / 2}
+            pr = {"rounds": 2, "main_iterations": 128, "primal_iterations": 64, "dual_iterations": 0,
+                  "main_seconds": 0.01, "polish_seconds": 0.001, "pair_relative_primal_residual": 0.0,
+                  "pair_relative_gap": s.eps_optimal / 2, "pair_primal_objective": -4.0,
+                  "main_relative_primal_residual": 1e-6, "main_relative_gap": float("nan")}
+            return 0, np.array([0.0, 2.0]), np.zeros(1), r, pr
+
+    out = b.polish_legs(_E(), _I, time_limit=1.0)
+    assert solves.count("close") == 2
+    assert [c for c in solves if c != "close"] == [("plain", 1e-4), ("polished", 1e-4), ("polished", 1e-6),
+                                                    ("plain", 1e-4), ("polished", 1e-4), ("polished", 1e-8)]
+    c1 = out["lp_config1"]
+    assert abs(c1["plain_1e-4"]["row_violation_rel"] - 0.1 / 3.0) < 1e-12
+    pol = c1["polished_gap_1e-04"]
+    assert pol["row_violation_rel"] == 0.0 and pol["rounds"] == 2 and pol["primal_polish_iterations"] == 64
+    assert abs(pol["objective_rel_err_vs_oracle"] - 1.0 / 4.0) < 1e-12
+    assert pol["main_at_last_handover"]["relative_gap"] is None    # NaN is not JSON
+    assert "polished_gap_1e-08" in out["lp_config0"]
+    json.dumps(out, allow_nan=False)
