@@ -1785,6 +1785,7 @@ int run_polished(const Scaled& sc, Core<double>& hi, const LoopParams& lp, const
         if (hi.run(ml, &ms)) return -1;
         pr->main_seconds += now_s() - t_main;
         main_used += ms.iterations;
+        pr->main_iterations = static_cast<int>(std::min<long long>(main_used, 2147483647LL));
         acc.iterations += ms.iterations;
         acc.restarts += ms.restarts;
         acc.syncs += ms.syncs;
@@ -1798,7 +1799,6 @@ int run_polished(const Scaled& sc, Core<double>& hi, const LoopParams& lp, const
         acc.cancelled = ms.cancelled;
         if (ms.numeric || ms.timed_out || ms.cancelled) break;
         ++pr->rounds;
-        pr->main_iterations = static_cast<int>(std::min<long long>(main_used, 2147483647LL));
         pr->main_relative_primal_residual = ms.best.primal;
         pr->main_relative_dual_residual = ms.best.dual;
         pr->main_relative_gap = ms.best.gap;
