@@ -48,7 +48,8 @@ def load(name: str) -> C.CDLL:
                 "ref_milp_hooked": os.path.join(HERE, "_ref", "libsankhya_ref_milp_hooked.so"),
                 "ref_lp": os.path.join(HERE, "_ref", "libsihps_lp_ref.so"),
                 "ref_lp_hooked": os.path.join(HERE, "_ref", "libsihps_lp_hooked.so"),
-                "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so")}[name]
+                "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so"),
+                "ref_crossover": os.path.join(HERE, "_ref", "libsk_crossover_ref.so")}[name]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")
         _libs[name] = C.CDLL(path)
@@ -584,3 +585,32 @@ def ref_sk_scale_model(inst, passes=4):
     r, c = np.zeros(inst["m"]), np.zeros(inst["n"])
     lib.sk_scale_model(C.byref(model), _p(r), _p(c), C.c_int(passes))
     return r, c
+
+
+class CrossoverStats(C.Structure):
+    """sk_b200_crossover_stats (include/integration/sk_crossover.h)."""
+    _fields_ = [("rounds", C.c_int), ("fixed_columns", C.c_int), ("released_columns", C.c_int),
+                ("full_fallback", C.c_int), ("simplex_iterations", C.c_longlong), ("seconds", C.c_double)]
+
+
+def ref_crossover(inst, x, y, fix_tolerance=1e-6, max_rounds=5, primal_tol=1e-7, dual_tol=1e-7):
+    """Runs the crossover integration source (built against the reference's C core) from
+    the first-order point (x, y); returns (status, dict with the certified x, y, the
+    sk_verify residuals and the crossover's counters)."""
+    lib = load("ref_crossover")
+    ref = load("ref")
+    keep = _Keep()
+    model = build_sk_model(keep, inst)
+    o = ref_options(primal_tol=primal_tol, dual_tol=dual_tol, lp_engine=0)
+    s = SkSolution()
+    ref.sk_solution_init(C.byref(s))
+    st = CrossoverStats()
+    rc = lib.sk_b200_crossover(C.byref(model), C.byref(o), _p(keep.d(x)), _p(keep.d(y)),
+                               C.c_double(fix_tolerance), C.c_int(max_rounds), C.byref(s), C.byref(st))
+    n, m = inst["n"], inst["m"]
+    out = {k: getattr(s, k) for k, _ in SkSolution._fields_ if k not in ("x", "y", "rc", "rowact")}
+    out.update({k: getattr(st, k) for k, _ in CrossoverStats._fields_})
+    out["x"] = np.ctypeslib.as_array(s.x, (n,)).copy() if s.x and n else np.zeros(n)
+    out["y"] = np.ctypeslib.as_array(s.y, (m,)).copy() if s.y and m else np.zeros(m)
+    ref.sk_solution_free(C.byref(s))
+    return rc, out
