@@ -49,7 +49,8 @@ def load(name: str) -> C.CDLL:
                 "ref_lp": os.path.join(HERE, "_ref", "libsihps_lp_ref.so"),
                 "ref_lp_hooked": os.path.join(HERE, "_ref", "libsihps_lp_hooked.so"),
                 "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so"),
-                "ref_crossover": os.path.join(HERE, "_ref", "libsk_crossover_ref.so")}[name]
+                "ref_crossover": os.path.join(HERE, "_ref", "libsk_crossover_ref.so"),
+                "ref_sihps_crossover": os.path.join(HERE, "_ref", "libsihps_crossover_ref.so")}[name]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")
         _libs[name] = C.CDLL(path)
@@ -613,4 +614,30 @@ def ref_crossover(inst, x, y, fix_tolerance=1e-6, max_rounds=5, primal_tol=1e-7,
     out["x"] = np.ctypeslib.as_array(s.x, (n,)).copy() if s.x and n else np.zeros(n)
     out["y"] = np.ctypeslib.as_array(s.y, (m,)).copy() if s.y and m else np.zeros(m)
     ref.sk_solution_free(C.byref(s))
+    return rc, out
+
+
+class RefCrossoverResult(C.Structure):
+    """RefCrossoverResult (oracle/ref_crossover_shim.cpp)."""
+    _fields_ = [("status", C.c_int), ("used_warm_start", C.c_int), ("dual_iterations", C.c_int),
+                ("cold_iterations", C.c_int), ("basic_structurals", C.c_int), ("repaired", C.c_int),
+                ("objective", C.c_double), ("primal_residual", C.c_double), ("dual_residual", C.c_double),
+                ("seconds", C.c_double)]
+
+
+def ref_sihps_crossover(inst, x, y):
+    """Runs the crossover source for the reference C++ core (a basis from the first-order
+    point (x, y) seated in its simplex); returns (rc, dict with x, y and the counters)."""
+    lib = load("ref_sihps_crossover")
+    keep = _Keep()
+    n, m = inst["n"], inst["m"]
+    x_out, y_out = np.zeros(n), np.zeros(m)
+    r = RefCrossoverResult()
+    rc = lib.ref_crossover_lp(C.c_int(m), C.c_int(n), C.c_int(int(inst["ptr"][-1])), _p(keep.i(inst["ptr"]), iptr),
+                              _p(keep.i(inst["idx"]), iptr), _p(keep.d(inst["val"])), _p(keep.d(inst["c"])),
+                              _p(keep.d(inst["cl"])), _p(keep.d(inst["cu"])), _p(keep.d(inst["rl"])),
+                              _p(keep.d(inst["ru"])), _p(keep.d(x)), _p(keep.d(y)), _p(x_out), _p(y_out),
+                              C.byref(r))
+    out = {k: getattr(r, k) for k, _ in RefCrossoverResult._fields_}
+    out["x"], out["y"] = x_out, y_out
     return rc, out

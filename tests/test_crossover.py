@@ -104,3 +104,73 @@ def test_argument_checks(oracle, instances):
     x, y = np.zeros(inst["n"]), np.zeros(inst["m"])
     assert oracle.ref_crossover(inst, x, y, fix_tolerance=0.0)[0] == 1   # SK_ERR_ARG
     assert oracle.ref_crossover(inst, x, y, max_rounds=0)[0] == 1
+
+
+# ---------------------------------------------------------------- the C++ core's simplex
+
+@pytest.fixture(scope="module")
+def sihps(oracle):
+    if not oracle.available("ref_sihps_crossover"):
+        pytest.skip("reference C++ core not built (make -C oracle ref)")
+    return oracle
+
+
+def gate(out, objective):
+    """OPTIMAL through the core's original-space gate (1e-6), at the simplex optimum."""
+    assert out["status"] == 0, out
+    assert out["primal_residual"] <= 1e-6 and out["dual_residual"] <= 1e-6, out
+    assert abs(out["objective"] - objective) <= 1e-9 * (1.0 + abs(objective)), (out["objective"], objective)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("eps", [1e-4, 1e-6, 1e-8])
+def test_seated_basis_from_pdlp_points(sihps, instances, name, eps):
+    """A basis identified from the PDLP restatement's point, seated in the core's simplex:
+    its warm path finishes it in a handful of dual pivots (the cold solve of lp300 takes
+    3,785 primal pivots)."""
+    inst = instances.lp_uniform(*CASES[name])
+    x, y, _ = sihps.pdlp(inst, eps=eps, max_iterations=400000)
+    rc, out = sihps.ref_sihps_crossover(inst, x, y)
+    assert rc == 0
+    gate(out, golden(name)["objective"])
+    assert out["used_warm_start"] == 1 and out["cold_iterations"] == 0, out
+    assert out["dual_iterations"] <= 50, out
+
+
+def test_seated_basis_config0(sihps, instances):
+    """Config 0 (2,000 x 5,000): from the 1e-6 point the warm dual simplex needs a few
+    pivots, where the core's cold simplex takes minutes (313.7 s measured on this LP)."""
+    inst = instances.lp_config0(0)
+    x, y, _ = sihps.pdlp(inst, eps=1e-6, max_iterations=400000)
+    rc, out = sihps.ref_sihps_crossover(inst, x, y)
+    assert rc == 0
+    gate(out, golden("lp_config0")["objective"])
+    assert out["used_warm_start"] == 1 and out["dual_iterations"] <= 50, out
+    assert out["seconds"] < 30.0, out
+
+
+def test_seated_basis_wrong_point_falls_back(sihps, instances):
+    """A point that names the wrong bounds: the core's gate refuses the warm answer or the
+    repair takes longer, and the answer is still the optimum."""
+    inst = instances.lp_uniform(*CASES["lp60"])
+    x, y, _ = sihps.pdlp(inst, eps=1e-6, max_iterations=400000)
+    rc, out = sihps.ref_sihps_crossover(inst, inst["cl"] + inst["cu"] - x, -y)
+    assert rc == 0
+    gate(out, golden("lp60")["objective"])
+
+
+def test_seated_basis_one_sided_columns(sihps, instances):
+    from scipy.optimize import linprog
+    import scipy.sparse as sp
+    inst = instances.lp_uniform(5, 80, 200, 4)
+    inst["cu"] = np.full(inst["n"], np.inf)
+    inst["cl"] = np.zeros(inst["n"])
+    inst["c"] = np.abs(inst["c"]) + 0.1
+    A = sp.csr_matrix((inst["val"], inst["idx"], inst["ptr"]), shape=(inst["m"], inst["n"]))
+    ref = linprog(inst["c"], A_ub=sp.vstack([A, -A]), b_ub=np.concatenate([inst["ru"], -inst["rl"]]),
+                  bounds=[(0, None)] * inst["n"], method="highs")
+    x, y, _ = sihps.pdlp(inst, eps=1e-6, max_iterations=400000)
+    rc, out = sihps.ref_sihps_crossover(inst, x, y)
+    assert rc == 0
+    gate(out, float(ref.fun))
+    assert out["used_warm_start"] == 1, out
