@@ -48,7 +48,7 @@ Columns by_column(const sihps::CSRMatrix& A) {
 }  // namespace
 
 sihps::LpResult crossover(const sihps::LpProblem& p, const std::vector<double>& x, const std::vector<double>& y,
-                          CrossoverStats* stats) {
+                          CrossoverStats* stats, double time_budget) {
     CrossoverStats local;
     CrossoverStats& st = stats ? *stats : local;
     st = CrossoverStats{};
@@ -170,6 +170,7 @@ sihps::LpResult crossover(const sihps::LpProblem& p, const std::vector<double>& 
     }
 
     sihps::Simplex simplex(p);
+    if (time_budget > 0.0) simplex.set_time_budget(time_budget);
     if (factored) simplex.set_warm_start_basis(&basis);
     sihps::LpResult r = simplex.solve();
     st.used_warm_start = r.used_warm_start;

@@ -33,9 +33,12 @@ struct CrossoverStats {
 };
 
 // problem: the LP in the core's form; x (n_cols) and y (n_rows): the first-order
-// point, y with rc = c + A'y (sk_solve's sign, the engine's). Returns the core's
-// LpResult (status, x, y_dual, objective and residuals in original units).
+// point, y with rc = c + A'y (sk_solve's sign, the engine's); time_budget: seconds for
+// the simplex (Simplex::set_time_budget; 0: none), after which it returns
+// ITERATION_LIMIT, as HYBRID's budgeted simplex does. Returns the core's LpResult
+// (status, x, y_dual, objective and residuals in original units).
 sihps::LpResult crossover(const sihps::LpProblem& problem, const std::vector<double>& x,
-                          const std::vector<double>& y, CrossoverStats* stats = nullptr);
+                          const std::vector<double>& y, CrossoverStats* stats = nullptr,
+                          double time_budget = 0.0);
 
 }  // namespace sihps_b200

@@ -625,9 +625,10 @@ class RefCrossoverResult(C.Structure):
                 ("seconds", C.c_double)]
 
 
-def ref_sihps_crossover(inst, x, y):
+def ref_sihps_crossover(inst, x, y, time_budget=0.0):
     """Runs the crossover source for the reference C++ core (a basis from the first-order
-    point (x, y) seated in its simplex); returns (rc, dict with x, y and the counters)."""
+    point (x, y) seated in its simplex, time_budget seconds for it, 0: none); returns
+    (rc, dict with x, y and the counters)."""
     lib = load("ref_sihps_crossover")
     keep = _Keep()
     n, m = inst["n"], inst["m"]
@@ -636,8 +637,8 @@ def ref_sihps_crossover(inst, x, y):
     rc = lib.ref_crossover_lp(C.c_int(m), C.c_int(n), C.c_int(int(inst["ptr"][-1])), _p(keep.i(inst["ptr"]), iptr),
                               _p(keep.i(inst["idx"]), iptr), _p(keep.d(inst["val"])), _p(keep.d(inst["c"])),
                               _p(keep.d(inst["cl"])), _p(keep.d(inst["cu"])), _p(keep.d(inst["rl"])),
-                              _p(keep.d(inst["ru"])), _p(keep.d(x)), _p(keep.d(y)), _p(x_out), _p(y_out),
-                              C.byref(r))
+                              _p(keep.d(inst["ru"])), _p(keep.d(x)), _p(keep.d(y)), C.c_double(time_budget),
+                              _p(x_out), _p(y_out), C.byref(r))
     out = {k: getattr(r, k) for k, _ in RefCrossoverResult._fields_}
     out["x"], out["y"] = x_out, y_out
     return rc, out

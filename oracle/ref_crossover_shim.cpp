@@ -29,7 +29,8 @@ typedef struct RefCrossoverResult {
 // the core throws.
 int ref_crossover_lp(int rows, int cols, int nnz, const int* ptr, const int* idx, const double* val,
                      const double* c, const double* cl, const double* cu, const double* rl, const double* ru,
-                     const double* x, const double* y, double* x_out, double* y_out, RefCrossoverResult* r) {
+                     const double* x, const double* y, double time_budget, double* x_out, double* y_out,
+                     RefCrossoverResult* r) {
     try {
         const double inf = std::numeric_limits<double>::infinity();
         const auto m = static_cast<std::size_t>(rows);
@@ -56,7 +57,7 @@ int ref_crossover_lp(int rows, int cols, int nnz, const int* ptr, const int* idx
         }
         sihps_b200::CrossoverStats st;
         const sihps::LpResult s = sihps_b200::crossover(p, std::vector<double>(x, x + cols),
-                                                        std::vector<double>(y, y + rows), &st);
+                                                        std::vector<double>(y, y + rows), &st, time_budget);
         r->status = static_cast<int>(s.status);
         r->used_warm_start = st.used_warm_start ? 1 : 0;
         r->dual_iterations = st.dual_iterations;

@@ -174,3 +174,14 @@ def test_seated_basis_one_sided_columns(sihps, instances):
     assert rc == 0
     gate(out, float(ref.fun))
     assert out["used_warm_start"] == 1, out
+
+
+def test_seated_basis_time_budget(sihps, instances):
+    """A budget the simplex cannot meet ends it with ITERATION_LIMIT (3), as HYBRID's
+    budgeted simplex does, instead of a cold solve without end."""
+    inst = instances.lp_uniform(*CASES["lp300"])
+    x, y, _ = sihps.pdlp(inst, eps=1e-6, max_iterations=400000)
+    rc, out = sihps.ref_sihps_crossover(inst, inst["cl"] + inst["cu"] - x, -y, time_budget=1e-9)
+    assert rc == 0 and out["status"] == 3, out
+    rc, out = sihps.ref_sihps_crossover(inst, x, y, time_budget=60.0)
+    assert rc == 0 and out["status"] == 0 and out["used_warm_start"] == 1, out
