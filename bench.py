@@ -452,6 +452,58 @@ def run_plain_pdhg(args):
     return 0
 
 
+def run_crossover(args):
+    """Config 0 to a certified vertex: the engine's FP64 restarted PDLP to 1e-6 (host
+    arrays, on the GPU), then the crossover sources run on the host with the
+    reference's own simplex codes (the C++ core's warm-started basis, and the C core's
+    held columns), each answer checked against the reference simplex's certified
+    optimum. The cold simplex times are the recorded ones of the same LP. Prints one
+    JSON line."""
+    E = _load("sankhya_b200", os.path.join(ROOT, "the-solver_b200", "__init__.py"))
+    I = _load("sankhya_b200_instances", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    print(json.dumps(crossover_legs(E, I, O)), flush=True)
+    return 0
+
+
+def crossover_legs(E, I, O, with_c_core=True):
+    """The legs of run_crossover for engine, instance and oracle modules."""
+    golden = json.load(open(os.path.join(ROOT, "tests", "golden", "simplex_lp_config0.json")))
+    opt = golden["objective"]
+    inst = I.lp_config0(0)
+    out = {"metric": "config 0 to a certified vertex: engine PDLP 1e-6, then crossover", "unit": "s",
+           "higher_is_better": False, "data": "synthetic", "dtype": "f64",
+           "workload": "lp_config0: m=2,000, n=5,000, 25,000 nnz",
+           "cold_simplex_recorded_s": {"c_core": golden.get("seconds"), "cpp_core": 313.7},
+           "oracle_objective": opt}
+    A = E.Matrix.from_instance(inst)
+    s = E.pdlp_default_settings()
+    s.eps_optimal, s.max_iterations, s.time_limit = 1e-6, 400000, 60.0
+    t0 = time.perf_counter()
+    rc, x, y, r = E.pdlp_solve(A, inst, s)
+    out["engine_pdlp"] = {"seconds": round(time.perf_counter() - t0, 4), "status": r["status"],
+                          "iterations": r["iterations"], "rc": rc}
+    A.close()
+    if rc != 0:
+        raise RuntimeError(E.last_error())
+    rel = lambda v: abs(v - opt) / (1.0 + abs(opt))
+    t0 = time.perf_counter()
+    xrc, xo = O.ref_sihps_crossover(inst, x, y, time_budget=600.0)
+    out["cpp_core_crossover"] = {"seconds": round(time.perf_counter() - t0, 3), "rc": xrc, "status": xo["status"],
+                                 "used_warm_start": xo["used_warm_start"], "dual_pivots": xo["dual_iterations"],
+                                 "cold_pivots": xo["cold_iterations"],
+                                 "objective_rel_err_vs_oracle": rel(xo["objective"])}
+    if with_c_core:
+        t0 = time.perf_counter()
+        src, so = O.ref_crossover(inst, x, y)
+        out["c_core_crossover"] = {"seconds": round(time.perf_counter() - t0, 3), "rc": src, "result": so["result"],
+                                   "pivots": so["simplex_iterations"], "held_columns": so["fixed_columns"],
+                                   "full_fallback": so["full_fallback"],
+                                   "objective_rel_err_vs_oracle": rel(so["objective"])}
+    return out
+
+
 def run_polish(args):
     """Feasibility polishing on config 1 (and config 0): the restarted FP64 PDLP
     stopped at 1e-4 relative KKT beside the polished solve (gap 1e-4, then 1e-6;
@@ -884,6 +936,8 @@ def main():
     ap.add_argument("--nodes-only", action="store_true", help="with --batches: the shared-matrix node batch only")
     ap.add_argument("--qp", action="store_true", help="convex QP workload instead of the headline line")
     ap.add_argument("--pdlp-compare", action="store_true", help="adaptive versus Halpern PDLP on four instances")
+    ap.add_argument("--crossover", action="store_true",
+                    help="config 0 to a certified vertex: engine PDLP, then the crossover sources")
     ap.add_argument("--polish", action="store_true",
                     help="feasibility polishing on configs 1 and 0 beside the plain restarted solve")
     ap.add_argument("--plain-pdhg", action="store_true",
@@ -893,6 +947,8 @@ def main():
         return run_plain_pdhg(args)
     if args.polish:
         return run_polish(args)
+    if args.crossover:
+        return run_crossover(args)
     if args.pdlp_compare:
         return run_pdlp_compare(args)
     if args.batches:

@@ -256,3 +256,41 @@ def test_polish_legs_report_plain_and_polished_answers(monkeypatch):
     assert pol["main_at_last_handover"]["relative_gap"] is None    # NaN is not JSON
     assert "polished_gap_1e-08" in out["lp_config0"]
     json.dumps(out, allow_nan=False)
+
+
+def test_crossover_leg_reaches_the_certified_vertex():
+    """The --crossover leg with a stand-in engine that answers with the oracle's PDLP
+    point (the engine's algorithm): the C++ core's seated basis gives the certified
+    config-0 optimum through its warm start."""
+    import pytest
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not (O.available("ref_sihps_crossover") and O.available("oracle")):
+        pytest.skip("reference cores not built (make -C oracle ref)")
+    b = _bench()
+    spec = importlib.util.spec_from_file_location("inst_for_bench", os.path.join(ROOT, "the-solver_b200", "instances.py"))
+    I = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(I)
+
+    class _E:
+        class Matrix:
+            @staticmethod
+            def from_instance(inst):
+                class _M:
+                    def close(self):
+                        pass
+                return _M()
+
+        def pdlp_default_settings(self):
+            return _Settings()
+
+        def pdlp_solve(self, A, inst, s):
+            x, y, st = O.pdlp(inst, eps=s.eps_optimal, max_iterations=s.max_iterations)
+            return 0, x, y, {"status": 0 if st["converged"] else 1, "iterations": st["iterations"]}
+
+    out = b.crossover_legs(_E(), I, O, with_c_core=False)
+    cpp = out["cpp_core_crossover"]
+    assert out["engine_pdlp"]["status"] == 0
+    assert cpp["rc"] == 0 and cpp["status"] == 0 and cpp["used_warm_start"] == 1, cpp
+    assert cpp["objective_rel_err_vs_oracle"] < 1e-9 and cpp["dual_pivots"] <= 50, cpp
+    json.dumps(out, allow_nan=False)
