@@ -283,7 +283,9 @@ typedef struct SankhyaB200PolishResult {
    from the main loop's x, run until its x meets polish_tolerance in relative
    primal residual, and the dual feasibility problem (every finite bound moved
    to 0, so that its dual feasible set is the original LP's) from the main
-   loop's y, run until its y meets polish_tolerance in relative dual residual.
+   loop's y, run until its y meets polish_tolerance in relative dual residual;
+   both are restarted PDHG with the constant step 0.9 / ||A||_2 and the main
+   loop's primal weight held, so each stays near its starting point.
    The pair (polished x, polished y) is scored on the original LP (result: its
    relative residuals, gap and objectives); when the pair misses a target (its
    gap above eps_optimal, or a polishing solve out of iterations) the main loop
