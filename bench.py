@@ -475,7 +475,7 @@ def crossover_legs(E, I, O, with_c_core=True):
     out = {"metric": "config 0 to a certified vertex: engine PDLP 1e-6, then crossover", "unit": "s",
            "higher_is_better": False, "data": "synthetic", "dtype": "f64",
            "workload": "lp_config0: m=2,000, n=5,000, 25,000 nnz",
-           "cold_simplex_recorded_s": {"c_core": golden.get("seconds"), "cpp_core": 313.7},
+           "cold_simplex_recorded_s": {"c_core": golden.get("seconds"), "cpp_core": 312.6},
            "oracle_objective": opt}
     A = E.Matrix.from_instance(inst)
     s = E.pdlp_default_settings()

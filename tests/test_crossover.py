@@ -139,7 +139,7 @@ def test_seated_basis_from_pdlp_points(sihps, instances, name, eps):
 
 def test_seated_basis_config0(sihps, instances):
     """Config 0 (2,000 x 5,000): from the 1e-6 point the warm dual simplex needs a few
-    pivots, where the core's cold simplex takes minutes (313.7 s measured on this LP)."""
+    pivots, where the core's cold simplex takes minutes (312.6 s measured on this LP)."""
     inst = instances.lp_config0(0)
     x, y, _ = sihps.pdlp(inst, eps=1e-6, max_iterations=400000)
     rc, out = sihps.ref_sihps_crossover(inst, x, y)
