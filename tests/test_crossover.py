@@ -185,3 +185,35 @@ def test_seated_basis_time_budget(sihps, instances):
     assert rc == 0 and out["status"] == 3, out
     rc, out = sihps.ref_sihps_crossover(inst, x, y, time_budget=60.0)
     assert rc == 0 and out["status"] == 0 and out["used_warm_start"] == 1, out
+
+
+@pytest.mark.parametrize("seed", [7, 8, 9, 10, 11])
+@pytest.mark.parametrize("shape", [(10, 14), (30, 45)])
+def test_mixed_row_and_column_types(sihps, seed, shape):
+    """E, G, L and ranged rows; free, upper-only, boxed and fixed columns (the LPs the
+    MPS tests write): both crossovers reach HiGHS's optimum, the C++ core's warm start
+    without a fallback."""
+    import sys
+    import scipy.sparse as sp
+    from scipy.optimize import linprog
+    sys.path.insert(0, os.path.dirname(__file__))
+    import mps_files
+    m, n = shape
+    inst = mps_files.lp_instance(seed, m, n)
+    A = sp.csr_matrix((inst["val"], inst["idx"], inst["ptr"]), shape=(m, n)).toarray()
+    eq = inst["rl"] == inst["ru"]
+    up, lo = ~eq & np.isfinite(inst["ru"]), ~eq & np.isfinite(inst["rl"])
+    G = np.vstack([A[up], -A[lo]])
+    h = np.concatenate([inst["ru"][up], -inst["rl"][lo]])
+    bounds = [(l if np.isfinite(l) else None, u if np.isfinite(u) else None) for l, u in zip(inst["cl"], inst["cu"])]
+    ref = linprog(inst["c"], A_ub=G, b_ub=h, A_eq=A[eq], b_eq=inst["rl"][eq], bounds=bounds, method="highs")
+    assert ref.status == 0
+    x, y, st = sihps.pdlp(inst, eps=1e-6, max_iterations=200000)
+    assert st["converged"]
+    rc, out = sihps.ref_crossover(inst, x, y)
+    assert rc == 0
+    certified(out, float(ref.fun))
+    rc, out = sihps.ref_sihps_crossover(inst, x, y)
+    assert rc == 0
+    gate(out, float(ref.fun))
+    assert out["used_warm_start"] == 1, out
