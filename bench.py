@@ -453,8 +453,8 @@ def run_plain_pdhg(args):
 
 
 def run_crossover(args):
-    """Config 0 to a certified vertex: the engine's FP64 restarted PDLP to 1e-6 (host
-    arrays, on the GPU), then the crossover sources run on the host with the
+    """Config 0 to a certified vertex: the engine's FP64 restarted PDLP to 1e-8 (config
+    0's target; host arrays, on the GPU), then the crossover sources run on the host with the
     reference's own simplex codes (the C++ core's warm-started basis, and the C core's
     held columns), each answer checked against the reference simplex's certified
     optimum. The cold simplex times are the recorded ones of the same LP. Prints one
@@ -472,14 +472,14 @@ def crossover_legs(E, I, O, with_c_core=True):
     golden = json.load(open(os.path.join(ROOT, "tests", "golden", "simplex_lp_config0.json")))
     opt = golden["objective"]
     inst = I.lp_config0(0)
-    out = {"metric": "config 0 to a certified vertex: engine PDLP 1e-6, then crossover", "unit": "s",
+    out = {"metric": "config 0 to a certified vertex: engine PDLP 1e-8, then crossover", "unit": "s",
            "higher_is_better": False, "data": "synthetic", "dtype": "f64",
            "workload": "lp_config0: m=2,000, n=5,000, 25,000 nnz",
            "cold_simplex_recorded_s": {"c_core": golden.get("seconds"), "cpp_core": 312.6},
            "oracle_objective": opt}
     A = E.Matrix.from_instance(inst)
     s = E.pdlp_default_settings()
-    s.eps_optimal, s.max_iterations, s.time_limit = 1e-6, 400000, 60.0
+    s.eps_optimal, s.max_iterations, s.time_limit = 1e-8, 400000, 60.0
     t0 = time.perf_counter()
     rc, x, y, r = E.pdlp_solve(A, inst, s)
     out["engine_pdlp"] = {"seconds": round(time.perf_counter() - t0, 4), "status": r["status"],
@@ -498,7 +498,8 @@ def crossover_legs(E, I, O, with_c_core=True):
         t0 = time.perf_counter()
         src, so = O.ref_crossover(inst, x, y)
         out["c_core_crossover"] = {"seconds": round(time.perf_counter() - t0, 3), "rc": src, "result": so["result"],
-                                   "pivots": so["simplex_iterations"], "held_columns": so["fixed_columns"],
+                                   "direct": so["direct"], "pivots": so["simplex_iterations"],
+                                   "held_columns": so["fixed_columns"],
                                    "full_fallback": so["full_fallback"],
                                    "objective_rel_err_vs_oracle": rel(so["objective"])}
     return out

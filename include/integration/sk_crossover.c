@@ -7,6 +7,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "sk_lu.h"
 #include "sk_simplex.h"
 
 enum { FREE_COL = 0, AT_LOW = 1, AT_UPP = 2 };
@@ -117,6 +118,133 @@ static sk_status assemble(const sk_model* m, const unsigned char* state, const s
     return sk_verify(m, out);
 }
 
+/* The basis the first-order point identifies, taken as it stands: of the ncol + nrow
+   columns of [A -I] (structurals, and the row logicals s = A x), the nrow with the
+   smallest reduced cost (|rc_j|; a logical's is |y_i|), ties to the farthest inside
+   their bounds, factorized with the core's sparse LU; its duals pi (B' pi = c_B) set
+   every nonbasic column at the bound that makes it dual feasible, the basic values
+   follow from B z_B = -N z_N, and sk_verify certifies the point (y = -pi in sk_solve's
+   sign). Returns 1 with out filled when the certificate holds; 0 otherwise (a singular
+   basis, or a basic value outside its bounds: the simplex has work to do). */
+typedef struct ranked {
+    double cost, inside;
+    int v;
+} ranked;
+
+static int by_rank(const void* a, const void* b)
+{
+    const ranked* p = (const ranked*)a;
+    const ranked* q = (const ranked*)b;
+    if (p->cost != q->cost) return p->cost < q->cost ? -1 : 1;
+    if (p->inside != q->inside) return p->inside > q->inside ? -1 : 1;
+    return p->v - q->v;
+}
+
+static int direct_basis(const sk_model* m, const sk_options* o, const double* x, const double* y, const double* rc,
+                        sk_solution* out)
+{
+    const int n = m->ncol, r = m->nrow, nv = n + r;
+    int ok = 0;
+    double* act = (double*)calloc((size_t)r + 1, sizeof(double));
+    double* value = (double*)malloc(sizeof(double) * (size_t)(nv + 1));
+    double* lo = (double*)malloc(sizeof(double) * (size_t)(nv + 1));
+    double* hi = (double*)malloc(sizeof(double) * (size_t)(nv + 1));
+    ranked* rank = (ranked*)malloc(sizeof(ranked) * (size_t)(nv + 1));
+    int* pos = (int*)malloc(sizeof(int) * (size_t)(nv + 1));       /* basis position or -1 */
+    double* pi = (double*)calloc((size_t)r + 1, sizeof(double));
+    double* z = (double*)calloc((size_t)r + 1, sizeof(double));
+    sk_csc B;
+    memset(&B, 0, sizeof(B));
+    B.p = (int*)malloc(sizeof(int) * (size_t)(r + 1));
+    B.i = (int*)malloc(sizeof(int) * (size_t)(m->A.p[n] + r + 1));
+    B.x = (double*)malloc(sizeof(double) * (size_t)(m->A.p[n] + r + 1));
+    sk_lu lu;
+    sk_lu_init(&lu);
+    if (!act || !value || !lo || !hi || !rank || !pos || !pi || !z || !B.p || !B.i || !B.x) goto done;
+
+    for (int j = 0; j < n; ++j)
+        for (int p = m->A.p[j]; p < m->A.p[j + 1]; ++p) act[m->A.i[p]] += m->A.x[p] * x[j];
+    for (int v = 0; v < nv; ++v) {
+        value[v] = v < n ? x[v] : act[v - n];
+        lo[v] = v < n ? m->clow[v] : m->rlow[v - n];
+        hi[v] = v < n ? m->cupp[v] : m->rupp[v - n];
+        double d = INFINITY;
+        if (!SK_IS_NEG_INF(lo[v])) d = fmin(d, (value[v] - lo[v]) / (1.0 + fabs(lo[v])));
+        if (!SK_IS_INF(hi[v])) d = fmin(d, (hi[v] - value[v]) / (1.0 + fabs(hi[v])));
+        rank[v].cost = fabs(v < n ? rc[v] : y[v - n]);
+        rank[v].inside = d;
+        rank[v].v = v;
+        pos[v] = -1;
+    }
+    qsort(rank, (size_t)nv, sizeof(ranked), by_rank);
+
+    /* B: structural columns of A, logical columns -e_i */
+    int nz = 0;
+    B.nrow = B.ncol = r;
+    B.p[0] = 0;
+    for (int k = 0; k < r; ++k) {
+        const int v = rank[k].v;
+        pos[v] = k;
+        if (v < n) {
+            for (int p = m->A.p[v]; p < m->A.p[v + 1]; ++p, ++nz) { B.i[nz] = m->A.i[p]; B.x[nz] = m->A.x[p]; }
+        } else {
+            B.i[nz] = v - n;
+            B.x[nz++] = -1.0;
+        }
+        B.p[k + 1] = nz;
+    }
+    B.nzmax = nz > 0 ? nz : 1;
+    if (sk_lu_factorize(&lu, &B, o->pivot_tol > 0.0 ? o->pivot_tol : 0.1) != SK_OK) goto done;
+    for (int k = 0; k < r; ++k) pi[k] = rank[k].v < n ? m->c[rank[k].v] : 0.0;
+    if (sk_lu_btran(&lu, pi) != SK_OK) goto done;
+
+    /* nonbasic columns at the bound their reduced cost d (c - A' pi; logicals pi_i) favours */
+    for (int v = 0; v < nv; ++v) {
+        if (pos[v] >= 0) continue;
+        double d;
+        if (v < n) {
+            d = m->c[v];
+            for (int p = m->A.p[v]; p < m->A.p[v + 1]; ++p) d -= m->A.x[p] * pi[m->A.i[p]];
+        } else {
+            d = pi[v - n];
+        }
+        const int lf = !SK_IS_NEG_INF(lo[v]), hf = !SK_IS_INF(hi[v]);
+        if (lf && hf) value[v] = d > 0.0 ? lo[v] : d < 0.0 ? hi[v] : (value[v] - lo[v] <= hi[v] - value[v] ? lo[v] : hi[v]);
+        else if (lf) value[v] = lo[v];
+        else if (hf) value[v] = hi[v];
+        else value[v] = 0.0;
+    }
+    /* B z_B = -N z_N over A x - s = 0 */
+    for (int v = 0; v < nv; ++v) {
+        if (pos[v] >= 0) continue;
+        if (v < n) {
+            for (int p = m->A.p[v]; p < m->A.p[v + 1]; ++p) z[m->A.i[p]] -= m->A.x[p] * value[v];
+        } else {
+            z[v - n] += value[v];
+        }
+    }
+    if (sk_lu_ftran(&lu, z) != SK_OK) goto done;
+    for (int k = 0; k < r; ++k) value[rank[k].v] = z[k];
+
+    out->x = (double*)malloc(sizeof(double) * (size_t)(n + 1));
+    out->y = (double*)malloc(sizeof(double) * (size_t)(r + 1));
+    out->rc = (double*)malloc(sizeof(double) * (size_t)(n + 1));
+    out->rowact = (double*)malloc(sizeof(double) * (size_t)(r + 1));
+    if (!out->x || !out->y || !out->rc || !out->rowact) goto done;
+    out->ncol = n;
+    out->nrow = r;
+    for (int j = 0; j < n; ++j) out->x[j] = value[j];
+    for (int i = 0; i < r; ++i) out->y[i] = -pi[i];
+    if (sk_verify(m, out) == SK_OK && out->primal_infeasibility <= o->primal_tol &&
+        out->dual_infeasibility <= o->dual_tol)
+        ok = 1;
+done:
+    sk_lu_free(&lu);
+    free(B.p); free(B.i); free(B.x);
+    free(act); free(value); free(lo); free(hi); free(rank); free(pos); free(pi); free(z);
+    return ok;
+}
+
 sk_status sk_b200_crossover(const sk_model* m, const sk_options* o, const double* x, const double* y,
                             double fix_tolerance, int max_rounds, sk_solution* out,
                             sk_b200_crossover_stats* stats)
@@ -133,8 +261,22 @@ sk_status sk_b200_crossover(const sk_model* m, const sk_options* o, const double
     double* rc = (double*)malloc(sizeof(double) * (size_t)(n + 1));
     if (!state || !rc) { free(state); free(rc); return SK_ERR_MEMORY; }
 
-    /* the bounds the first-order point selects */
     reduced_costs(m, y, rc);
+    /* the identified basis as it stands: no simplex when the point was accurate enough */
+    sk_solution_free(out);
+    if (direct_basis(m, o, x, y, rc, out)) {
+        free(state);
+        free(rc);
+        stats->direct = 1;
+        out->result = SK_RESULT_OPTIMAL;
+        out->iterations = 0;
+        stats->seconds = sk_wall_seconds() - t0;
+        out->solve_seconds = stats->seconds;
+        return SK_OK;
+    }
+    sk_solution_free(out);
+
+    /* the bounds the first-order point selects */
     const double window = sqrt(fix_tolerance);
     for (int j = 0; j < n; ++j) {
         const int lo = !SK_IS_NEG_INF(m->clow[j]), hi = !SK_IS_INF(m->cupp[j]);

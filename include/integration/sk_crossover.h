@@ -12,7 +12,11 @@
    by sk_verify on the whole model. A fixed column whose reduced cost at the
    new duals has the wrong sign for its bound is released and the smaller LP
    solved again; when nothing is left to release, or after max_rounds solves,
-   the whole model goes to the simplex from its usual start. */
+   the whole model goes to the simplex from its usual start. Before any of that,
+   the basis the point identifies (the nrow columns of [A -I] with the smallest
+   reduced costs, nonbasic columns at the bounds its own duals favour, factorized
+   with the core's sparse LU) is tried as it stands: when sk_verify certifies it,
+   no simplex runs. */
 #ifndef SK_B200_CROSSOVER_H
 #define SK_B200_CROSSOVER_H
 
@@ -27,6 +31,8 @@ typedef struct sk_b200_crossover_stats {
     int fixed_columns;            /* columns fixed in the last smaller LP                */
     int released_columns;         /* fixed columns released over all rounds              */
     int full_fallback;            /* 1: the whole model was solved from the usual start  */
+    int direct;                   /* 1: the basis the point identifies was certified as it
+                                     stands, without a simplex solve                       */
     long long simplex_iterations; /* over every simplex solve                            */
     double seconds;
 } sk_b200_crossover_stats;

@@ -591,7 +591,8 @@ def ref_sk_scale_model(inst, passes=4):
 class CrossoverStats(C.Structure):
     """sk_b200_crossover_stats (include/integration/sk_crossover.h)."""
     _fields_ = [("rounds", C.c_int), ("fixed_columns", C.c_int), ("released_columns", C.c_int),
-                ("full_fallback", C.c_int), ("simplex_iterations", C.c_longlong), ("seconds", C.c_double)]
+                ("full_fallback", C.c_int), ("direct", C.c_int), ("simplex_iterations", C.c_longlong),
+                ("seconds", C.c_double)]
 
 
 def ref_crossover(inst, x, y, fix_tolerance=1e-6, max_rounds=5, primal_tol=1e-7, dual_tol=1e-7):

@@ -260,8 +260,9 @@ def test_polish_legs_report_plain_and_polished_answers(monkeypatch):
 
 def test_crossover_leg_reaches_the_certified_vertex():
     """The --crossover leg with a stand-in engine that answers with the oracle's PDLP
-    point (the engine's algorithm): the C++ core's seated basis gives the certified
-    config-0 optimum through its warm start."""
+    point (the engine's algorithm) at config 0's 1e-8: the C++ core's seated basis gives
+    the certified optimum through its warm start, and the C core's identified basis is
+    certified as it stands (no simplex)."""
     import pytest
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -288,9 +289,13 @@ def test_crossover_leg_reaches_the_certified_vertex():
             x, y, st = O.pdlp(inst, eps=s.eps_optimal, max_iterations=s.max_iterations)
             return 0, x, y, {"status": 0 if st["converged"] else 1, "iterations": st["iterations"]}
 
-    out = b.crossover_legs(_E(), I, O, with_c_core=False)
-    cpp = out["cpp_core_crossover"]
+    if not O.available("ref_crossover"):
+        pytest.skip("reference C core not built (make -C oracle ref)")
+    out = b.crossover_legs(_E(), I, O)
+    cpp, cc = out["cpp_core_crossover"], out["c_core_crossover"]
     assert out["engine_pdlp"]["status"] == 0
     assert cpp["rc"] == 0 and cpp["status"] == 0 and cpp["used_warm_start"] == 1, cpp
     assert cpp["objective_rel_err_vs_oracle"] < 1e-9 and cpp["dual_pivots"] <= 50, cpp
+    assert cc["rc"] == 0 and cc["result"] == 0 and cc["direct"] == 1 and cc["pivots"] == 0, cc
+    assert cc["objective_rel_err_vs_oracle"] < 1e-9, cc
     json.dumps(out, allow_nan=False)

@@ -39,14 +39,20 @@ def certified(out, objective):
 @pytest.mark.parametrize("eps", [1e-4, 1e-6, 1e-8])
 def test_from_pdlp_points(oracle, instances, name, eps):
     """From the PDLP restatement's point at 1e-4, 1e-6 and 1e-8: the certified simplex
-    optimum, with columns fixed and fewer simplex iterations than the cold solve."""
+    optimum, either from the identified basis as it stands (no simplex; always from the
+    1e-8 point) or with columns held and fewer simplex iterations than the cold solve."""
     inst = instances.lp_uniform(*CASES[name])
     g = golden(name)
     x, y, _ = oracle.pdlp(inst, eps=eps, max_iterations=400000)
     rc, out = oracle.ref_crossover(inst, x, y)
     assert rc == 0
     certified(out, g["objective"])
-    assert out["full_fallback"] == 0 and out["fixed_columns"] > 0, out
+    if out["direct"]:
+        assert out["simplex_iterations"] == 0 and out["rounds"] == 0, out
+    else:
+        assert out["full_fallback"] == 0 and out["fixed_columns"] > 0, out
+    if eps <= 1e-8:
+        assert out["direct"] == 1, out
     assert out["simplex_iterations"] < g["iterations"], (out["simplex_iterations"], g["iterations"])
     assert out["iterations"] == out["simplex_iterations"]
 
@@ -217,3 +223,15 @@ def test_mixed_row_and_column_types(sihps, seed, shape):
     assert rc == 0
     gate(out, float(ref.fun))
     assert out["used_warm_start"] == 1, out
+
+
+def test_config0_identified_basis_is_certified(oracle, instances):
+    """Config 0 from its target tolerance (1e-8): the basis the point identifies is the
+    optimal vertex as it stands; sk_verify certifies it with no simplex solve, where the
+    cold simplex of the C core takes 876.8 s and 74,059 pivots."""
+    inst = instances.lp_config0(0)
+    x, y, _ = oracle.pdlp(inst, eps=1e-8, max_iterations=400000)
+    rc, out = oracle.ref_crossover(inst, x, y)
+    assert rc == 0
+    certified(out, golden("lp_config0")["objective"])
+    assert out["direct"] == 1 and out["simplex_iterations"] == 0, out
