@@ -235,3 +235,31 @@ def test_config0_identified_basis_is_certified(oracle, instances):
     assert rc == 0
     certified(out, golden("lp_config0")["objective"])
     assert out["direct"] == 1 and out["simplex_iterations"] == 0, out
+
+
+# the reference's PDLP known-answer LPs (tests/lp/test_pdlp.cpp:53-150), whose optimal
+# vertices are stated there
+INF = float("inf")
+HAND = [
+    (dict(rows=3, cols=2, dense=[1, 0, 0, 2, 3, 2], c=[-3, -5], rl=[-INF] * 3, ru=[4, 12, 18], cl=[0, 0],
+          cu=[INF, INF]), [2.0, 6.0], -36.0),
+    (dict(rows=1, cols=1, dense=[1], c=[-1], rl=[2], ru=[7], cl=[0], cu=[100]), [7.0], -7.0),
+    (dict(rows=1, cols=2, dense=[1, 1], c=[-1, -1], rl=[-INF], ru=[100], cl=[0, 0], cu=[3, 4]), [3.0, 4.0], -7.0),
+]
+
+
+@pytest.mark.parametrize("case", range(len(HAND)))
+def test_known_answer_vertices(sihps, instances, case):
+    """The reference's own known answers: both crossovers return the stated vertex exactly
+    (to the simplex's accuracy) from the PDLP restatement's 1e-6 point."""
+    spec, vertex, objective = HAND[case]
+    inst = instances.small_dense_lp(**spec)
+    x, y, _ = sihps.pdlp(inst, eps=1e-6, max_iterations=100000)
+    rc, out = sihps.ref_crossover(inst, x, y)
+    assert rc == 0
+    certified(out, objective)
+    assert np.allclose(out["x"], vertex, atol=1e-9), out["x"]
+    rc, out = sihps.ref_sihps_crossover(inst, x, y)
+    assert rc == 0
+    gate(out, objective)
+    assert np.allclose(out["x"], vertex, atol=1e-9), out["x"]
