@@ -87,13 +87,19 @@ sihps::LpResult crossover(const sihps::LpProblem& p, const std::vector<double>& 
         inside[v] = d;
     }
 
-    // the basis: smallest |reduced cost| first, ties to the most interior
+    // the basis: smallest |reduced cost| first, ties to the most interior; a caller with
+    // no dual (y all zero, e.g. an answer that kept only x) ranks by interiority alone
+    bool have_dual = false;
+    for (std::int32_t i = 0; i < m && !have_dual; ++i) have_dual = y[static_cast<std::size_t>(i)] != 0.0;
     std::vector<std::int32_t> order(unv);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](std::int32_t a, std::int32_t b) {
-        const double ra = std::fabs(red[static_cast<std::size_t>(a)]), rb = std::fabs(red[static_cast<std::size_t>(b)]);
-        if (ra != rb) return ra < rb;
-        return inside[static_cast<std::size_t>(a)] > inside[static_cast<std::size_t>(b)];
+        const auto ua = static_cast<std::size_t>(a), ub = static_cast<std::size_t>(b);
+        if (have_dual) {
+            const double ra = std::fabs(red[ua]), rb = std::fabs(red[ub]);
+            if (ra != rb) return ra < rb;
+        }
+        return inside[ua] > inside[ub];
     });
     sihps::Simplex::Basis basis;
     basis.n_struct = n;

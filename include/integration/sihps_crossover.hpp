@@ -33,7 +33,9 @@ struct CrossoverStats {
 };
 
 // problem: the LP in the core's form; x (n_cols) and y (n_rows): the first-order
-// point, y with rc = c + A'y (sk_solve's sign, the engine's); time_budget: seconds for
+// point, y with rc = c + A'y (sk_solve's sign, the engine's; all zero when the caller
+// kept only x, as run_first_order does: the basis is then ranked by interiority alone);
+// time_budget: seconds for
 // the simplex (Simplex::set_time_budget; 0: none), after which it returns
 // ITERATION_LIMIT, as HYBRID's budgeted simplex does. Returns the core's LpResult
 // (status, x, y_dual, objective and residuals in original units).

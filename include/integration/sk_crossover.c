@@ -161,6 +161,9 @@ static int direct_basis(const sk_model* m, const sk_options* o, const double* x,
     sk_lu lu;
     sk_lu_init(&lu);
     if (!act || !value || !lo || !hi || !rank || !pos || !pi || !z || !B.p || !B.i || !B.x) goto done;
+    /* a caller with no dual (y all zero) ranks by interiority alone */
+    int have_dual = 0;
+    for (int i = 0; i < r && !have_dual; ++i) have_dual = y[i] != 0.0;
 
     for (int j = 0; j < n; ++j)
         for (int p = m->A.p[j]; p < m->A.p[j + 1]; ++p) act[m->A.i[p]] += m->A.x[p] * x[j];
@@ -171,7 +174,7 @@ static int direct_basis(const sk_model* m, const sk_options* o, const double* x,
         double d = INFINITY;
         if (!SK_IS_NEG_INF(lo[v])) d = fmin(d, (value[v] - lo[v]) / (1.0 + fabs(lo[v])));
         if (!SK_IS_INF(hi[v])) d = fmin(d, (hi[v] - value[v]) / (1.0 + fabs(hi[v])));
-        rank[v].cost = fabs(v < n ? rc[v] : y[v - n]);
+        rank[v].cost = have_dual ? fabs(v < n ? rc[v] : y[v - n]) : 0.0;
         rank[v].inside = d;
         rank[v].v = v;
         pos[v] = -1;

@@ -40,7 +40,8 @@ typedef struct sk_b200_crossover_stats {
 /* m: an LP (no Q, objsense 1, as sk_solve's models are); o: the simplex options
    (primal_tol / dual_tol also bound the certificate); x (ncol) and y (nrow): the
    first-order point, y in sk_solve's sign convention (rc = c + A'y, a row at its
-   lower bound has y <= 0); fix_tolerance > 0: a column is fixed when |rc_j| exceeds
+   lower bound has y <= 0; all zero when only x is at hand, the identified basis then
+   ranked by interiority alone); fix_tolerance > 0: a column is fixed when |rc_j| exceeds
    it and x_j lies within sqrt(fix_tolerance) (1 + |bound|) of the bound its sign
    selects; max_rounds >= 1; out initialised by sk_solution_init. On SK_OK, out holds
    x, y, rc and rowact of the certified vertex (free with sk_solution_free), its

@@ -263,3 +263,22 @@ def test_known_answer_vertices(sihps, instances, case):
     assert rc == 0
     gate(out, objective)
     assert np.allclose(out["x"], vertex, atol=1e-9), out["x"]
+
+
+@pytest.mark.parametrize("name", ["lp300", "lp_config0"])
+def test_from_x_alone(sihps, instances, name):
+    """A caller that kept only x (run_first_order returns x alone) passes y = 0: the basis
+    is ranked by interiority, and both crossovers still reach the certified optimum, the
+    C++ core through its warm start, the C core from the 1e-8 point with no simplex."""
+    inst = instances.lp_uniform(*CASES[name]) if name in CASES else instances.lp_config0(0)
+    g = golden(name)
+    x, y, _ = sihps.pdlp(inst, eps=1e-8, max_iterations=400000)
+    zero = np.zeros_like(y)
+    rc, out = sihps.ref_sihps_crossover(inst, x, zero, time_budget=120.0)
+    assert rc == 0
+    gate(out, g["objective"])
+    assert out["used_warm_start"] == 1 and out["dual_iterations"] <= 50, out
+    rc, out = sihps.ref_crossover(inst, x, zero)
+    assert rc == 0
+    certified(out, g["objective"])
+    assert out["direct"] == 1, out
