@@ -57,15 +57,32 @@ def spliced(text: str, body: str) -> str:
     return out.replace(anchor, anchor + '#include "sankhya_b200.h"\n', 1)
 
 
+def spliced_hybrid(text: str, body: str) -> str:
+    """LpSolver.cpp with the `try_simplex` lambda of solve_lp's HYBRID branch replaced by
+    `body` (include/integration/lpsolver_hybrid_crossover.inc) and the crossover header
+    added after the file's own includes."""
+    start = text.index("        auto try_simplex = [&]() {")
+    end = text.index("\n        };\n", start) + len("\n        };\n")
+    out = text[:start] + body + text[end:]
+    anchor = '#include "Scaling.hpp"\n'
+    if anchor not in out:
+        raise ValueError("LpSolver.cpp: include anchor not found")
+    return out.replace(anchor, anchor + '#include "sihps_crossover.hpp"\n', 1)
+
+
 def _run(cmd, **kw):
     r = subprocess.run(cmd, capture_output=True, text=True, **kw)
     if r.returncode != 0:
         raise RuntimeError(" ".join(cmd[:4]) + " ...\n" + r.stderr[-3000:])
 
 
-def build(ref: str, out: str, hook: bool, lib_dir: str | None = None, rpath: str | None = None) -> str:
+def build(ref: str, out: str, hook: bool, lib_dir: str | None = None, rpath: str | None = None,
+          hybrid_crossover: bool = False) -> str:
+    """hybrid_crossover (with hook): HYBRID's simplex step replaced as well, by
+    include/integration/lpsolver_hybrid_crossover.inc, with sihps_crossover.cpp compiled in."""
     src = os.path.join(ref, "src")
-    inc = ["-I" + src, "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(CUDA, "include")]
+    integration = os.path.join(ROOT, "include", "integration")
+    inc = ["-I" + src, "-I" + os.path.join(ROOT, "include"), "-I" + integration, "-I" + os.path.join(CUDA, "include")]
     tmp = tempfile.mkdtemp(prefix="sihps_lp_")
     try:
         def compile_one(rel):
@@ -83,8 +100,15 @@ def build(ref: str, out: str, hook: bool, lib_dir: str | None = None, rpath: str
         lp_obj = os.path.join(tmp, "lp_LpSolver.cpp.o")
         text = open(os.path.join(src, "lp", "LpSolver.cpp")).read()
         if hook:
+            source = spliced(text, block())
+            if hybrid_crossover:
+                source = spliced_hybrid(source, open(os.path.join(integration, "lpsolver_hybrid_crossover.inc")).read())
+                xobj = os.path.join(tmp, "sihps_crossover.o")
+                _run(["g++", "-O3", "-DNDEBUG", "-std=c++17", "-fPIC"] + inc +
+                     ["-c", os.path.join(integration, "sihps_crossover.cpp"), "-o", xobj])
+                objs.append(xobj)
             _run(["g++", "-O3", "-DNDEBUG", "-std=c++17", "-fPIC", "-iquote", os.path.join(src, "lp")] + inc +
-                 ["-x", "c++", "-", "-c", "-o", lp_obj], input=spliced(text, block()))
+                 ["-x", "c++", "-", "-c", "-o", lp_obj], input=source)
         else:
             _run(["g++", "-O3", "-DNDEBUG", "-std=c++17", "-fPIC"] + inc + ["-c", os.path.join(src, "lp", "LpSolver.cpp"),
                                                                              "-o", lp_obj])
@@ -108,11 +132,13 @@ def main(argv=None) -> int:
     ap.add_argument("--hook", action="store_true")
     ap.add_argument("--lib-dir", default=None)
     ap.add_argument("--rpath", default=None, help="run-time search path for the engine library")
+    ap.add_argument("--hybrid-crossover", action="store_true",
+                    help="with --hook: HYBRID's simplex step through the crossover as well")
     a = ap.parse_args(argv)
     if a.hook and not a.lib_dir:
         ap.error("--hook needs --lib-dir")
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
-    build(a.ref, a.out, a.hook, a.lib_dir, a.rpath)
+    build(a.ref, a.out, a.hook, a.lib_dir, a.rpath, a.hybrid_crossover)
     return 0
 
 

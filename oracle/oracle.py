@@ -50,7 +50,9 @@ def load(name: str) -> C.CDLL:
                 "ref_lp_hooked": os.path.join(HERE, "_ref", "libsihps_lp_hooked.so"),
                 "ref_cuda": os.path.join(HERE, "_ref", "libsankhya_cuda_ref.so"),
                 "ref_crossover": os.path.join(HERE, "_ref", "libsk_crossover_ref.so"),
-                "ref_sihps_crossover": os.path.join(HERE, "_ref", "libsihps_crossover_ref.so")}[name]
+                "ref_sihps_crossover": os.path.join(HERE, "_ref", "libsihps_crossover_ref.so"),
+                "ref_lp_cpu": os.path.join(HERE, "_ref", "libsihps_lp_cpu.so"),
+                "ref_lp_hybrid_cpu": os.path.join(HERE, "_ref", "libsihps_lp_hybrid_cpu.so")}[name]
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} is not built (make -C oracle {'ref' if name != 'oracle' else ''})")
         _libs[name] = C.CDLL(path)
@@ -321,13 +323,15 @@ LP_SIMPLEX, LP_FIRST_ORDER, LP_HYBRID = 0, 1, 2
 LP_STATUS = ("OPTIMAL", "INFEASIBLE", "UNBOUNDED", "ITERATION_LIMIT", "NUMERICAL_FAILURE")
 
 
-def ref_solve_lp(inst, method=LP_SIMPLEX, hooked=False, **opts):
+def ref_solve_lp(inst, method=LP_SIMPLEX, hooked=False, lib_name=None, **opts):
     """The reference C++ core's sihps::solve_lp (src/lp/LpSolver.cpp:126-334) on the
     instance: (x, result dict). `hooked` selects the build whose run_first_order is the
     integration block calling the engine; otherwise FIRST_ORDER runs the reference's own
-    GpuPdlp. Keyword options are RefLpOptions fields; the rest keep the core's defaults.
-    SIMPLEX runs on the CPU; FIRST_ORDER and HYBRID need a GPU."""
-    lib = load("ref_lp_hooked" if hooked else "ref_lp")
+    GpuPdlp. `lib_name` picks another build ("ref_lp_cpu", "ref_lp_hybrid_cpu": the
+    integration blocks over the CPU stand-in engine). Keyword options are RefLpOptions
+    fields; the rest keep the core's defaults. SIMPLEX runs on the CPU; FIRST_ORDER and
+    HYBRID need a GPU, except through the stand-in builds."""
+    lib = load(lib_name or ("ref_lp_hooked" if hooked else "ref_lp"))
     o = RefLpOptions()
     lib.ref_lp_default_options(C.byref(o))
     o.method = method

@@ -282,3 +282,43 @@ def test_from_x_alone(sihps, instances, name):
     assert rc == 0
     certified(out, g["objective"])
     assert out["direct"] == 1, out
+
+
+# ------------------------------------------- HYBRID's simplex step through the crossover
+
+@pytest.fixture(scope="module")
+def stand_in(oracle):
+    if not (oracle.available("ref_lp_cpu") and oracle.available("ref_lp_hybrid_cpu")):
+        pytest.skip("LP driver builds over the CPU stand-in engine absent (make -C oracle ref-tests)")
+    return oracle
+
+
+def test_hybrid_fallback_through_the_crossover(stand_in, instances):
+    """The reference's own LP driver, run_first_order spliced in (the engine's entry points
+    answered on the CPU by the oracle's PDLP): its first-order answer converges but does not
+    pass the driver's 1e-6 original-space gate, so HYBRID hands the model to the simplex.
+    Without the crossover block that simplex starts cold (thousands of pivots); with it
+    (include/integration/lpsolver_hybrid_crossover.inc) it starts from the basis the
+    first-order x identifies and needs none. Same certified optimum either way."""
+    inst = instances.lp_uniform(*CASES["lp300"])
+    g = golden("lp300")["objective"]
+    opts = dict(method=stand_in.LP_HYBRID, hybrid_row_threshold=1, pdlp_max_iterations=200000,
+                hybrid_first_order_eps=1e-6)
+    _, cold = stand_in.ref_solve_lp(inst, lib_name="ref_lp_cpu", **opts)
+    _, warm = stand_in.ref_solve_lp(inst, lib_name="ref_lp_hybrid_cpu", **opts)
+    for r in (cold, warm):
+        assert r["status_name"] == "OPTIMAL" and r["pdlp_converged"] == 1 and r["used_first_order"] == 0, r
+        assert abs(r["objective"] - g) <= 1e-9 * (1.0 + abs(g)) and r["primal_residual"] <= 1e-6, r
+    assert cold["iterations"] > 1000 and warm["iterations"] <= 50, (cold, warm)
+
+
+def test_hybrid_simplex_leading_is_unchanged(stand_in, instances):
+    """When the simplex leads (row count below the threshold) nothing has iterated before
+    it, so the crossover block leaves it cold: the same pivots as without the block."""
+    inst = instances.lp_uniform(*CASES["lp60"])
+    opts = dict(method=stand_in.LP_HYBRID, hybrid_row_threshold=10 ** 9)
+    x0, a = stand_in.ref_solve_lp(inst, lib_name="ref_lp_cpu", **opts)
+    x1, b = stand_in.ref_solve_lp(inst, lib_name="ref_lp_hybrid_cpu", **opts)
+    assert a["status_name"] == b["status_name"] == "OPTIMAL"
+    assert a["iterations"] == b["iterations"] and a["pdlp_iterations"] == b["pdlp_iterations"] == 0
+    assert np.array_equal(x0, x1)

@@ -82,6 +82,29 @@ def test_a_wrong_field_is_caught(lp_solver_source):
     assert r.returncode != 0 and "host_sync_count" in r.stderr
 
 
+def test_hybrid_crossover_compiles_in_place(lp_solver_source):
+    """HYBRID's simplex step replaced by the crossover block (with run_first_order
+    replaced as above): the spliced LpSolver.cpp compiles against the core's Simplex,
+    LpResult and PdlpStats and the crossover header."""
+    import hooked_lpsolver
+    ref, text = lp_solver_source
+    body = open(os.path.join(INTEGRATION, "lpsolver_hybrid_crossover.inc")).read()
+    assert "sihps_b200::crossover(" in body
+    source = hooked_lpsolver.spliced_hybrid(_spliced(text, _block()), body)
+    assert source.count("\n        auto try_simplex = [&]() {\n") == 1 and "sihps_crossover.hpp" in source
+    lp = os.path.join(ref, "src", "lp")
+    cmd = ["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Werror=return-type", "-iquote", lp,
+           "-I" + os.path.join(ref, "src"), "-I" + os.path.join(ROOT, "include"), "-I" + INTEGRATION,
+           "-I/usr/local/cuda/include", "-x", "c++", "-"]
+    r = subprocess.run(cmd, input=source, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    broken = body.replace("crossover_stats, options.hybrid_simplex_budget_seconds",
+                          "crossover_stats, options.hybrid_simplex_budget")
+    r = subprocess.run(cmd, input=hooked_lpsolver.spliced_hybrid(_spliced(text, _block()), broken),
+                       capture_output=True, text=True)
+    assert r.returncode != 0 and "hybrid_simplex_budget" in r.stderr
+
+
 MILP_WRAPPER = """
 #include "sankhya_b200.h"
 #include <string.h>
