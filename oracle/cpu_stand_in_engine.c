@@ -3,8 +3,9 @@
  * sankhya_b200_pdlp_default_settings, sankhya_b200_pdlp_solve), answering with the
  * oracle's restatement of the restarted PDLP (orc_pdlp, no scaling). It lets the
  * reference's own LP driver, with the integration blocks spliced in, run its
- * first-order paths on a machine without a GPU: built as libsankhya_cuda.so in a
- * directory of its own (oracle/_ref/cpu_stand_in/) and linked in the engine's place.
+ * first-order paths on a machine without a GPU: built as libsankhya_cuda_cpu_stand_in.so
+ * (a name of its own, so that a process holding both never mistakes one for the other;
+ * oracle/_ref/cpu_stand_in/) and linked in the engine's place.
  * The product never links it. */
 #include <stdlib.h>
 #include <string.h>

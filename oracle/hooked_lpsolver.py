@@ -77,9 +77,10 @@ def _run(cmd, **kw):
 
 
 def build(ref: str, out: str, hook: bool, lib_dir: str | None = None, rpath: str | None = None,
-          hybrid_crossover: bool = False) -> str:
+          hybrid_crossover: bool = False, engine_lib: str = "sankhya_cuda") -> str:
     """hybrid_crossover (with hook): HYBRID's simplex step replaced as well, by
-    include/integration/lpsolver_hybrid_crossover.inc, with sihps_crossover.cpp compiled in."""
+    include/integration/lpsolver_hybrid_crossover.inc, with sihps_crossover.cpp compiled in.
+    engine_lib: the library the hook links (lib<engine_lib>.so in lib_dir)."""
     src = os.path.join(ref, "src")
     integration = os.path.join(ROOT, "include", "integration")
     inc = ["-I" + src, "-I" + os.path.join(ROOT, "include"), "-I" + integration, "-I" + os.path.join(CUDA, "include")]
@@ -118,7 +119,7 @@ def build(ref: str, out: str, hook: bool, lib_dir: str | None = None, rpath: str
             "-L" + os.path.join(CUDA, "lib64"), "-lcusparse", "-lcudart",
             "-Xlinker", "-rpath", "-Xlinker", os.path.join(CUDA, "lib64"), "-Xlinker", "--no-undefined"]
         if hook:
-            link += ["-L" + lib_dir, "-lsankhya_cuda", "-Xlinker", "-rpath", "-Xlinker", rpath or lib_dir]
+            link += ["-L" + lib_dir, "-l" + engine_lib, "-Xlinker", "-rpath", "-Xlinker", rpath or lib_dir]
         _run(link)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
@@ -134,11 +135,12 @@ def main(argv=None) -> int:
     ap.add_argument("--rpath", default=None, help="run-time search path for the engine library")
     ap.add_argument("--hybrid-crossover", action="store_true",
                     help="with --hook: HYBRID's simplex step through the crossover as well")
+    ap.add_argument("--engine-lib", default="sankhya_cuda", help="with --hook: the library name to link")
     a = ap.parse_args(argv)
     if a.hook and not a.lib_dir:
         ap.error("--hook needs --lib-dir")
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
-    build(a.ref, a.out, a.hook, a.lib_dir, a.rpath, a.hybrid_crossover)
+    build(a.ref, a.out, a.hook, a.lib_dir, a.rpath, a.hybrid_crossover, a.engine_lib)
     return 0
 
 
