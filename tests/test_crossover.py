@@ -322,3 +322,14 @@ def test_hybrid_simplex_leading_is_unchanged(stand_in, instances):
     assert a["status_name"] == b["status_name"] == "OPTIMAL"
     assert a["iterations"] == b["iterations"] and a["pdlp_iterations"] == b["pdlp_iterations"] == 0
     assert np.array_equal(x0, x1)
+
+
+def test_infeasible_lp_is_reported_not_certified(sihps, instances):
+    """x0 + x1 in [5, 6] with x in [0, 2]^2 has no solution: no basis is certified; the
+    C core's fallback simplex and the C++ core's warm dual simplex both prove infeasibility."""
+    inst = instances.small_dense_lp(rows=1, cols=2, dense=[1, 1], c=[1, 1], rl=[5], ru=[6], cl=[0, 0], cu=[2, 2])
+    x, y = np.array([2.0, 2.0]), np.array([-1.0])
+    rc, out = sihps.ref_crossover(inst, x, y)
+    assert rc == 0 and out["result"] == 1 and out["direct"] == 0 and out["full_fallback"] == 1, out   # INFEASIBLE
+    rc, out = sihps.ref_sihps_crossover(inst, x, y)
+    assert rc == 0 and out["status"] == 1, out                                                          # INFEASIBLE
