@@ -333,3 +333,17 @@ def test_infeasible_lp_is_reported_not_certified(sihps, instances):
     assert rc == 0 and out["result"] == 1 and out["direct"] == 0 and out["full_fallback"] == 1, out   # INFEASIBLE
     rc, out = sihps.ref_sihps_crossover(inst, x, y)
     assert rc == 0 and out["status"] == 1, out                                                          # INFEASIBLE
+
+
+def test_unbounded_lp_is_reported_not_certified(sihps, instances):
+    """min -x0 with x0 - x1 <= 1, x >= 0 is unbounded: no basis is certified, and both
+    cores' fallbacks report UNBOUNDED (the C++ core's warm start is refused, no dual
+    feasible basis existing)."""
+    inf = float("inf")
+    inst = instances.small_dense_lp(rows=1, cols=2, dense=[1, -1], c=[-1, 0], rl=[-inf], ru=[1], cl=[0, 0],
+                                    cu=[inf, inf])
+    x, y = np.array([5.0, 4.0]), np.array([0.5])
+    rc, out = sihps.ref_crossover(inst, x, y)
+    assert rc == 0 and out["result"] == 2 and out["full_fallback"] == 1, out    # UNBOUNDED
+    rc, out = sihps.ref_sihps_crossover(inst, x, y)
+    assert rc == 0 and out["status"] == 2 and out["used_warm_start"] == 0, out  # UNBOUNDED
